@@ -1,0 +1,93 @@
+// gb_common.cuh -- shared device-side definitions of the garli_b200 engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gb {
+
+constexpr int kRescaleTableLen = 90;  // RESCALE_ARRAY_LENGTH, tree.h:48
+constexpr int kMaxLevelOps = 96;      // CLA ops per batched launch (kernel-parameter bound)
+constexpr int kMaxScoreBlocks = 4096; // partial-sum slots for the edge reduction
+constexpr int kThreads = 256;
+
+enum OpKind : int { kIntInt = 0, kIntTip = 1, kTipTip = 2 };
+enum StatusBits : int { kStatusRescaleRetry = 1, kStatusNonFinite = 2 };
+
+// One CLA update after host normalisation: c1 is the internal child whenever
+// exactly one child is a tip (Tree::UpdateCLAs, tree.cpp:3905-3990, swaps the
+// children the same way when calling CalcFullCLAInternalTerminal).
+struct DevOp {
+    int dest, c1, p1, c2, p2;
+    int kind;
+    int rescale;  // plain form: rank >= rescaleEvery (tree.cpp:3991)
+};
+
+struct LevelOps {
+    int n;
+    DevOp op[kMaxLevelOps];
+};
+
+// Device view of an instance, passed by value to every kernel.
+struct View {
+    void *partials;           // nbuf x cla_stride elements (double or float)
+    int *scalers;             // nbuf x npat_pad
+    const uint8_t *tips;      // ntip x npat_pad
+    const double *mats;       // nmat x mat_stride: [P | dP | d2P], each R*S*S
+    const int *counts;        // npat_pad (0 in the padding)
+    const int *const_states;  // npat_pad
+    const double *freqs;      // S
+    const double *rate_probs; // R
+    int *status;
+    double *block_sums;       // kMaxScoreBlocks x 3
+    double *site_lnl;         // npat_pad
+    long long cla_stride;     // elements per CLA buffer = npat_pad * R * S
+    long long mat_stride;     // 3 * R * S * S
+    int npat, npat_pad, ntip, last_const, has_pinv, rescale_every;
+    double pinv;
+};
+
+// rescale tables (tree.cpp:163-172), filled from the host with the same libm
+// (defined here: the engine is a single CUDA translation unit)
+__constant__ double c_thresh[kRescaleTableLen];
+__constant__ double c_mult[kRescaleTableLen];
+__constant__ int c_incr[kRescaleTableLen];
+__constant__ double c_rescale_below, c_reduce_below, c_bail_below;
+
+// Strict IEEE arithmetic: GARLI's CPU build evaluates these expressions without
+// fused multiply-add, so the plain form spells every operation out.
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+template <typename ST>
+__device__ __forceinline__ void load4(const ST *p, double v[4]);
+template <>
+__device__ __forceinline__ void load4<double>(const double *p, double v[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+template <>
+__device__ __forceinline__ void load4<float>(const float *p, double v[4]) {
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+template <typename ST>
+__device__ __forceinline__ void store4(ST *p, const double v[4]);
+template <>
+__device__ __forceinline__ void store4<double>(double *p, const double v[4]) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+template <>
+__device__ __forceinline__ void store4<float>(float *p, const double v[4]) {
+    reinterpret_cast<float4 *>(p)[0] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+}
+
+// lanes per pattern for R rate categories (a power of two dividing 32)
+template <int R>
+struct Lanes {
+    static constexpr int G = R <= 1 ? 1 : R <= 2 ? 2 : R <= 4 ? 4 : 8;
+};
+
+}  // namespace gb

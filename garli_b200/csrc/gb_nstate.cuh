@@ -1,0 +1,246 @@
+// gb_nstate.cuh -- 20-state (amino acid) and 61-state (codon) kernels.
+//
+// CUDA-core FP64 versions that keep GARLI's per-site arithmetic order
+// (sequential sums over "to" states, tree.cpp:7843-7910, :8537-8600,
+// :5597-6460, optimization.cpp:2592-3614).  A block owns a tile of TP
+// patterns; the two P(t) sets of the op and the children's tiles are staged
+// in shared memory, each thread produces (pattern, from-state) outputs, and
+// the tile of results stays in shared memory until the per-pattern rescale
+// decision has been taken.
+#pragma once
+#include "gb_common.cuh"
+
+namespace gb {
+
+template <typename ST>
+__device__ __forceinline__ double ldv(const ST *p) { return (double)__ldg(p); }
+
+// dynamic shared memory layout for k_cla_ns:
+//   PL[R*S*S], PR[R*S*S], A[TP*R*S], B[TP*R*S], D[TP*R*S], mx[TP], mlt[TP]
+template <typename ST, bool GARLI_SCALE>
+__global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S, int R, int TP) {
+    extern __shared__ double sm[];
+    const DevOp op = ops.op[blockIdx.y];
+    const int RS = R * S, RSS = R * S * S;
+    double *PL = sm, *PR = PL + RSS, *A = PR + RSS, *B = A + TP * RS, *D = B + TP * RS;
+    double *mx = D + TP * RS;
+    const double *m1 = v.mats + (long long)op.p1 * v.mat_stride;
+    const double *m2 = v.mats + (long long)op.p2 * v.mat_stride;
+    for (int i = threadIdx.x; i < RSS; i += blockDim.x) {
+        PL[i] = m1[i];
+        PR[i] = m2[i];
+    }
+    const int p0 = blockIdx.x * TP;
+    const int np = min(TP, v.npat - p0);
+    const ST *base = reinterpret_cast<const ST *>(v.partials);
+    if (op.kind != kTipTip) {
+        const ST *ca = base + (long long)op.c1 * v.cla_stride + (long long)p0 * RS;
+        for (int i = threadIdx.x; i < np * RS; i += blockDim.x) A[i] = ldv<ST>(ca + i);
+    }
+    if (op.kind == kIntInt) {
+        const ST *cb = base + (long long)op.c2 * v.cla_stride + (long long)p0 * RS;
+        for (int i = threadIdx.x; i < np * RS; i += blockDim.x) B[i] = ldv<ST>(cb + i);
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
+        const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
+        const int p = p0 + pl;
+        const double *pl_row = PL + r * S * S + from * S;
+        const double *pr_row = PR + r * S * S + from * S;
+        double val;
+        if (op.kind == kIntInt) {
+            const double *a = A + pl * RS + r * S, *b = B + pl * RS + r * S;
+            double L1 = 0.0, R1 = 0.0;
+            for (int to = 0; to < S; to++) {
+                L1 = add(L1, mul(pl_row[to], a[to]));
+                R1 = add(R1, mul(pr_row[to], b[to]));
+            }
+            val = mul(L1, R1);
+        } else if (op.kind == kIntTip) {
+            const double *a = A + pl * RS + r * S;
+            double acc = 0.0;
+            for (int to = 0; to < S; to++) acc = add(acc, mul(pl_row[to], a[to]));
+            const int s2 = v.tips[(long long)op.c2 * v.npat_pad + p];
+            val = (s2 < S) ? mul(acc, pr_row[s2]) : acc;
+        } else {
+            const int l = v.tips[(long long)op.c1 * v.npat_pad + p];
+            const int rr = v.tips[(long long)op.c2 * v.npat_pad + p];
+            const double tl = (l < S) ? pl_row[l] : 1.0;
+            const double tr = (rr < S) ? pr_row[rr] : 1.0;
+            val = mul(tl, tr);
+        }
+        D[o] = val;
+    }
+    __syncthreads();
+    // per-pattern largest entry (RescaleRateHetNState, tree.cpp:3492-3598)
+    for (int pl = threadIdx.x; pl < np; pl += blockDim.x) {
+        double large = D[pl * RS] > D[pl * RS + 1] ? D[pl * RS] : D[pl * RS + 1];
+        for (int s = 2; s < RS; s++) large = D[pl * RS + s] > large ? D[pl * RS + s] : large;
+        const int p = p0 + pl;
+        int m = 0;
+        if (op.kind == kIntInt) m = v.scalers[(long long)op.c1 * v.npat_pad + p] + v.scalers[(long long)op.c2 * v.npat_pad + p];
+        else if (op.kind == kIntTip) m = v.scalers[(long long)op.c1 * v.npat_pad + p];
+        double mult = 1.0;
+        if (GARLI_SCALE) {
+            if (op.rescale && large < c_rescale_below) {
+                if (large < c_reduce_below && (v.rescale_every > 2 || large < c_bail_below))
+                    atomicOr(v.status, kStatusRescaleRetry);
+                int idx = 0;
+                while ((idx + 1) < kRescaleTableLen && c_thresh[idx + 1] > large) idx++;
+                mult = c_mult[idx];
+                m += c_incr[idx];
+            }
+        } else if (large > 0.0) {
+            const int e = ilogb(large);
+            mult = ldexp(1.0, -e);
+            m -= e;
+        }
+        mx[pl] = mult;
+        v.scalers[(long long)op.dest * v.npat_pad + p] = m;
+    }
+    __syncthreads();
+    ST *dst = reinterpret_cast<ST *>(v.partials) + (long long)op.dest * v.cla_stride + (long long)p0 * RS;
+    for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
+        const double mult = mx[o / RS];
+        double val = D[o];
+        if (mult != 1.0) val = mul(val, mult);
+        dst[o] = (ST)val;
+    }
+}
+
+// Edge evaluation for S states: per-(pattern, rate, from) terms computed in
+// parallel, then summed per pattern in the reference's order.
+// dynamic smem: M[3*R*S*S], C[TP*R*S], Pp[TP*R*S], T[3*TP*R*S], freqs[S], rp[R]
+template <typename ST, bool GARLI_SCALE, bool DERIV>
+__global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf, int mat, int child_tip,
+                                                      int write_sites, int S, int R, int TP) {
+    extern __shared__ double sm[];
+    const int RS = R * S, RSS = R * S * S;
+    double *M = sm, *C = M + 3 * RSS, *Pp = C + TP * RS, *T = Pp + TP * RS, *F = T + 3 * TP * RS, *RP = F + S;
+    const double *mp = v.mats + (long long)mat * v.mat_stride;
+    for (int i = threadIdx.x; i < (DERIV ? 3 : 1) * RSS; i += blockDim.x) M[i] = mp[i];
+    for (int i = threadIdx.x; i < S; i += blockDim.x) F[i] = v.freqs[i];
+    for (int i = threadIdx.x; i < R; i += blockDim.x) RP[i] = v.rate_probs[i];
+    const ST *base = reinterpret_cast<const ST *>(v.partials);
+    double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int p0 = blockIdx.x * TP; p0 < v.npat; p0 += gridDim.x * TP) {
+        const int np = min(TP, v.npat - p0);
+        __syncthreads();
+        {
+            const ST *pa = base + (long long)pbuf * v.cla_stride + (long long)p0 * RS;
+            for (int i = threadIdx.x; i < np * RS; i += blockDim.x) Pp[i] = ldv<ST>(pa + i);
+            if (!child_tip) {
+                const ST *ca = base + (long long)cbuf * v.cla_stride + (long long)p0 * RS;
+                for (int i = threadIdx.x; i < np * RS; i += blockDim.x) C[i] = ldv<ST>(ca + i);
+            }
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
+            const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
+            const int p = p0 + pl;
+            const double *row = M + r * S * S + from * S;
+            double l = 0.0, a = 0.0, b = 0.0;
+            if (!child_tip) {
+                const double *c = C + pl * RS + r * S;
+                for (int to = 0; to < S; to++) {
+                    l = add(l, mul(row[to], c[to]));
+                    if (DERIV) {
+                        a = add(a, mul(row[RSS + to], c[to]));
+                        b = add(b, mul(row[2 * RSS + to], c[to]));
+                    }
+                }
+            } else {
+                const int s = v.tips[(long long)cbuf * v.npat_pad + p];
+                if (s < S) {
+                    l = row[s];
+                    if (DERIV) {
+                        a = row[RSS + s];
+                        b = row[2 * RSS + s];
+                    }
+                } else {
+                    l = 1.0;  // total ambiguity: partial*freq only, no derivative terms
+                }
+            }
+            const double w = Pp[pl * RS + r * S + from];
+            const bool amb = child_tip && v.tips[(long long)cbuf * v.npat_pad + p] >= S;
+            // reference: temp * partial[from] * freqs[from]  (ambiguous tip: partial[from] * freqs[from])
+            T[o] = amb ? mul(w, F[from]) : mul(mul(l, w), F[from]);
+            if (DERIV) {
+                T[TP * RS + o] = mul(mul(a, w), F[from]);
+                T[2 * TP * RS + o] = mul(mul(b, w), F[from]);
+            }
+        }
+        __syncthreads();
+        for (int pl = threadIdx.x; pl < np; pl += blockDim.x) {
+            const int p = p0 + pl;
+            double siteL = 0.0, sD1 = 0.0, sD2 = 0.0;
+            if (R == 1) {
+                for (int from = 0; from < S; from++) {
+                    siteL = add(siteL, T[pl * RS + from]);
+                    if (DERIV) {
+                        sD1 = add(sD1, T[TP * RS + pl * RS + from]);
+                        sD2 = add(sD2, T[2 * TP * RS + pl * RS + from]);
+                    }
+                }
+                siteL = mul(siteL, RP[0]);
+                if (DERIV) {
+                    sD1 = mul(sD1, RP[0]);
+                    sD2 = mul(sD2, RP[0]);
+                }
+            } else {
+                for (int r = 0; r < R; r++) {
+                    double rL = 0.0, r1 = 0.0, r2 = 0.0;
+                    for (int from = 0; from < S; from++) {
+                        rL = add(rL, T[pl * RS + r * S + from]);
+                        if (DERIV) {
+                            r1 = add(r1, T[TP * RS + pl * RS + r * S + from]);
+                            r2 = add(r2, T[2 * TP * RS + pl * RS + r * S + from]);
+                        }
+                    }
+                    siteL = add(siteL, mul(rL, RP[r]));
+                    if (DERIV) {
+                        sD1 = add(sD1, mul(r1, RP[r]));
+                        sD2 = add(sD2, mul(r2, RP[r]));
+                    }
+                }
+            }
+            const int m1 = v.scalers[(long long)pbuf * v.npat_pad + p];
+            const int m2 = child_tip ? 0 : v.scalers[(long long)cbuf * v.npat_pad + p];
+            if (v.has_pinv && p <= v.last_const) {
+                const double pf = mul(v.pinv, F[v.const_states[p]]);
+                if (GARLI_SCALE) {
+                    if (DERIV) {
+                        // prI*freq*exp(partial)*exp(child) (optimization.cpp:3300, :3507)
+                        siteL = child_tip ? add(siteL, mul(pf, exp((double)m1)))
+                                          : add(siteL, mul(mul(pf, exp((double)m1)), exp((double)m2)));
+                    } else if (m1 + m2 == 0) {
+                        siteL = add(siteL, pf);
+                    } else {
+                        siteL = add(siteL, mul(pf, exp(add((double)m1, (double)m2))));
+                    }
+                } else {
+                    siteL = add(siteL, ldexp(pf, m1 + m2));
+                }
+            }
+            double u;
+            if (GARLI_SCALE) u = sub(sub(log(siteL), (double)m1), (double)m2);
+            else u = sub(log(siteL), (double)(m1 + m2) * 0.69314718055994530941723212145818);
+            if (write_sites) v.site_lnl[p] = u;
+            // GARLI drops non-negative site lnLs (tree.cpp:6380, optimization.cpp:3378)
+            if (u < 0.0) {
+                const double cnt = (double)v.counts[p];
+                accL = add(accL, mul(u, cnt));
+                if (DERIV) {
+                    const double d1 = sD1 / siteL;
+                    const double d2 = sub(sD2 / siteL, mul(d1, d1));
+                    acc1 = add(acc1, mul(cnt, d1));
+                    acc2 = add(acc2, mul(cnt, d2));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    block_sum3(accL, acc1, acc2, v.block_sums + 3 * blockIdx.x);
+}
+
+}  // namespace gb

@@ -1,0 +1,97 @@
+// gb_pmat.cuh -- FP64 transition matrices and the final FP64 reduction.
+#pragma once
+#include "gb_common.cuh"
+
+namespace gb {
+
+constexpr int kMaxTransOps = 64;
+
+struct TransOp {
+    int dest;
+    int eigen;
+    int derivs;
+    double t;
+};
+struct TransOps {
+    int n;
+    TransOp op[kMaxTransOps];
+};
+
+// P(t), dP/dt, d2P/dt2 for every rate category, one block per matrix:
+//   Model::AltCalcPmat   model.cpp:1469-1597
+//   Model::CalcDerivatives model.cpp:1271-1358
+// scaledEigVal = lambda * rate [/(1-pinv)]; e_k = exp(scaledEigVal * t);
+// P_ij = max(0, sum_k (U_ik Uinv_kj) e_k) with the k sum sequential.
+// eig layout per eigen index: [lambda (S) | U (S*S) | Uinv (S*S)], lambda pre-scaled
+// by the blen multiplier.
+__global__ void __launch_bounds__(kThreads) k_pmats(const double *eig, long long eig_stride, int S, int R,
+                                                    const double *rates, double pinv, int has_pinv,
+                                                    TransOps ops, double *mats, long long mat_stride) {
+    const TransOp op = ops.op[blockIdx.x];
+    extern __shared__ double sh[];
+    double *ex = sh, *d1e = ex + R * S, *d2e = d1e + R * S;
+    const double *lam = eig + (long long)op.eigen * eig_stride;
+    const double *U = lam + S, *Ui = U + S * S;
+    for (int idx = threadIdx.x; idx < R * S; idx += blockDim.x) {
+        const int r = idx / S, k = idx % S;
+        double sev = mul(lam[k], rates[r]);
+        if (has_pinv) sev = sev / sub(1.0, pinv);
+        const double e = exp(mul(sev, op.t));
+        ex[idx] = e;
+        d1e[idx] = mul(sev, e);
+        d2e[idx] = mul(sev, d1e[idx]);
+    }
+    __syncthreads();
+    double *out = mats + (long long)op.dest * mat_stride;
+    const int SS = S * S;
+    for (int idx = threadIdx.x; idx < R * SS; idx += blockDim.x) {
+        const int r = idx / SS, ij = idx % SS, i = ij / S, j = ij % S;
+        const double *e = ex + r * S;
+        double sp = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int k = 0; k < S; k++) {
+            const double x = mul(U[i * S + k], Ui[k * S + j]);
+            sp = add(sp, mul(x, e[k]));
+            if (op.derivs) {
+                s1 = add(s1, mul(x, d1e[r * S + k]));
+                s2 = add(s2, mul(x, d2e[r * S + k]));
+            }
+        }
+        out[idx] = sp > 0.0 ? sp : 0.0;
+        if (op.derivs) {
+            out[R * SS + idx] = s1;
+            out[2 * R * SS + idx] = s2;
+        }
+    }
+}
+
+// Sum the per-block partial sums of an edge evaluation (nblocks x 3) into
+// out[0..2].  One block; each thread adds a fixed strided subset in order and
+// the block combines them in a fixed tree, so the result is deterministic.
+__global__ void __launch_bounds__(kThreads) k_reduce3(const double *parts, int nblocks, double *out) {
+    __shared__ double s[3][kThreads];
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+        a += parts[3 * i];
+        b += parts[3 * i + 1];
+        c += parts[3 * i + 2];
+    }
+    s[0][threadIdx.x] = a;
+    s[1][threadIdx.x] = b;
+    s[2][threadIdx.x] = c;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            s[0][threadIdx.x] += s[0][threadIdx.x + w];
+            s[1][threadIdx.x] += s[1][threadIdx.x + w];
+            s[2][threadIdx.x] += s[2][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = s[0][0];
+        out[1] = s[1][0];
+        out[2] = s[2][0];
+    }
+}
+
+}  // namespace gb

@@ -1,0 +1,219 @@
+/*
+ * garli_b200.h -- C ABI of the B200 likelihood engine for GARLI.
+ *
+ * The engine replaces the compute backend under GARLI's CalculationManager
+ * (garli/trunk/src/calculationmanager.h, subsetcalculationmanager.cpp), i.e.
+ * the beagle-lib calls GARLI issues today, with hand-written sm_100a kernels.
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (GB_SUCCESS or a negative GB_ERROR_* code) and is synchronous from the
+ * caller's point of view unless documented otherwise, exactly like the
+ * beagle calls it replaces (calculationmanager.cpp:84-125 maps those codes).
+ *
+ * Index spaces (calculationmanager.h:1147-1215):
+ *   buffer index b in [0, tipCount) ............ tip b (GARLI taxon number b+1)
+ *   buffer index b in [tipCount, tipCount+partialsBufferCount) .. a CLA buffer;
+ *                                                 its scaler array shares the index
+ *   matrix index m in [0, matrixBufferCount) .... a P(t) matrix set (P, dP/dt, d2P/dt2)
+ *   eigen index e in [0, eigenBufferCount) ...... an eigensystem of Q
+ */
+#ifndef GARLI_B200_H
+#define GARLI_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (beagle-compatible meaning, BEAGLE_ERROR_*) ---- */
+#define GB_SUCCESS 0
+#define GB_ERROR_GENERAL (-1)
+#define GB_ERROR_OUT_OF_MEMORY (-2)
+#define GB_ERROR_UNIDENTIFIED_EXCEPTION (-3)
+#define GB_ERROR_UNINITIALIZED_INSTANCE (-4)
+#define GB_ERROR_OUT_OF_RANGE (-5)
+#define GB_ERROR_NO_RESOURCE (-6)
+#define GB_ERROR_NO_IMPLEMENTATION (-7)
+#define GB_ERROR_FLOATING_POINT (-8)
+/* GARLI's throw(1) from RescaleRateHet (tree.cpp:3442,3448): a site fell below
+ * 1e-190 between rescalings; the caller lowers rescaleEvery by 2, dirties all
+ * CLAs and rescores (tree.cpp:4077-4090). */
+#define GB_ERROR_RESCALE_RETRY (-9)
+#define GB_ERROR_NO_DEVICE (-10)
+
+/* ---- instance flags ---- */
+/* plain form: FP64 CLAs with GARLI's rank-gated, e-based integer rescaling
+ * (tree.cpp:149-172, :3370); reproduces GARLI's CPU lnL and scaler counts */
+#define GB_FLAG_PLAIN_FP64 (1L << 0)
+/* precision form: FP32 CLA storage, per-site power-of-two rescaling after
+ * every CLA update (int32 exponent counts), FP64 P(t), sums and Newton step */
+#define GB_FLAG_MIXED_FP32 (1L << 1)
+
+typedef struct {
+    int resourceNumber; /* CUDA device ordinal */
+    long flags;         /* the GB_FLAG_* form in use */
+    int paddedPatterns; /* patterns rounded up to the kernel tile */
+    long long deviceBytes;
+    char deviceName[64];
+} gb_instance_details;
+
+/* ClaOperation, calculationmanager.h:39-52.  Child indices are buffer indices
+ * (tips or CLA buffers); the matrix indices select the P(t) of each child's
+ * branch.  opDepLevel orders the operations: every op of level k only reads
+ * buffers written at levels < k (or clean buffers). */
+typedef struct {
+    int destClaIndex;
+    int childClaIndex1;
+    int childClaIndex2;
+    int transMatIndex1;
+    int transMatIndex2;
+    int opDepLevel;
+} gb_cla_operation;
+
+/* TransMatOperation, calculationmanager.h:54-67 */
+typedef struct {
+    int destTransMatIndex;
+    double edgeLength;
+    int eigenIndex; /* modelIndex in GARLI: selects the eigensystem */
+    int calcDerivs; /* also fill dP/dt and d2P/dt2 (model.cpp:1271) */
+} gb_transmat_operation;
+
+/* ScoringOperation, calculationmanager.h:91-105: the partial CLA on one side
+ * of a branch, the child buffer on the other side, and that branch's matrix. */
+typedef struct {
+    int destClaIndex;   /* unused by the engine (GARLI passes the final scaler slot) */
+    int childClaIndex1; /* "partial": always a CLA buffer */
+    int childClaIndex2; /* child: tip or CLA buffer */
+    int transMatIndex;
+    int derivatives;    /* also return d1 and d2 (optimization.cpp:1099) */
+} gb_scoring_operation;
+
+/* ---- instance management (beagleCreateInstance / beagleFinalizeInstance) ---- */
+int gb_get_device_count(void);
+/* subsetcalculationmanager.cpp:105 beagleCreateInstance; stateCount 4, 20 or 61,
+ * categoryCount 1..8.  Returns an instance handle (>= 0) or an error code. */
+int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, int patternCount,
+                       int eigenBufferCount, int matrixBufferCount, int categoryCount,
+                       int resourceNumber, long flags, gb_instance_details *details);
+int gb_finalize_instance(int instance);
+
+/* ---- data (subsetcalculationmanager.cpp:177-230) ---- */
+/* beagleSetTipStates: DNA codes are 4-bit masks (A=1,C=2,G=4,T=8, 15 = missing,
+ * sequencedata.cpp:672); NState codes are state indices, stateCount = missing. */
+int gb_set_tip_states(int instance, int tipIndex, const unsigned char *codes);
+/* beagleSetPatternWeights: integer pattern counts (datamatr.cpp PatternManager) */
+int gb_set_pattern_weights(int instance, const int *counts);
+/* constant patterns 0..lastConst and their states (datamatr.cpp:334-376);
+ * needed for the +I term of GetScorePartial* (tree.cpp:6118-6130) */
+int gb_set_constant_patterns(int instance, int lastConst, const int *constStates);
+
+/* ---- model (subsetcalculationmanager.cpp:232-300, :765-800) ---- */
+int gb_set_state_frequencies(int instance, const double *freqs);
+/* beagleSetCategoryRates: GARLI's rateMults (model.cpp:2170) */
+int gb_set_category_rates(int instance, const double *rates);
+/* beagleSetCategoryWeights: GARLI's rateProbs = (1-pinv)/ncat (model.cpp:2199) */
+int gb_set_category_weights(int instance, const double *weights);
+/* proportion of invariant sites; hasPinv=0 reproduces NoPinvInModel() */
+int gb_set_invariant_sites(int instance, double pinv, int hasPinv);
+/* beagleSetEigenDecomposition: U (row-major S*S), U^-1, eigenvalues already
+ * multiplied by GARLI's blen_multiplier (model.cpp:845) */
+int gb_set_eigen_decomposition(int instance, int eigenIndex, const double *eigenVectors,
+                               const double *inverseEigenVectors, const double *eigenValues);
+
+/* ---- operations ---- */
+/* beagleUpdateTransitionMatrices (subsetcalculationmanager.cpp:232): P(t) and,
+ * if requested, dP/dt and d2P/dt2 in FP64 on the device (model.cpp:1271,:1469) */
+int gb_update_transition_matrices(int instance, const gb_transmat_operation *ops, int count);
+/* beagleSetTransitionMatrix: host-supplied FP64 P (row-major [cat][from][to]) */
+int gb_set_transition_matrix(int instance, int matrixIndex, const double *P, const double *D1,
+                             const double *D2);
+/* beagleUpdatePartials + beagleAccumulateScaleFactors
+ * (subsetcalculationmanager.cpp:595-640).  Operations are executed level by
+ * level (opDepLevel, ascending); ops of one level run in one batched launch.
+ * In the plain form the engine applies GARLI's rescale rule per destination
+ * buffer: rank = 2 (tip-tip), child+2 (internal-tip), 2+L+R (internal-internal),
+ * rescale when rank >= rescaleEvery (tree.cpp:3991, :7665-8598).  Asynchronous:
+ * a GB_ERROR_RESCALE_RETRY condition is reported by the next call that
+ * returns results. */
+int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int rescaleEvery);
+/* beagleCalculateEdgeLogLikelihoods (subsetcalculationmanager.cpp:765-901):
+ * returns lnL and, when op->derivatives, d1 and d2 in outLnL[0..2]. */
+int gb_calculate_edge(int instance, const gb_scoring_operation *op, double *out);
+/* beagleGetSiteLogLikelihoods of the last gb_calculate_edge (unscaled per pattern) */
+int gb_get_site_log_likelihoods(int instance, double *out);
+/* debug read-back (beagleGetPartials / beagleGetScaleFactors); CLA layout
+ * [pattern][category][state], converted to FP64 */
+int gb_get_partials(int instance, int bufferIndex, double *out);
+int gb_get_scale_factors(int instance, int bufferIndex, int *out);
+int gb_get_transition_matrix(int instance, int matrixIndex, int which, double *out);
+/* rescale rank the engine tracks for a CLA buffer (condlike.h rescaleRank) */
+int gb_get_rescale_rank(int instance, int bufferIndex);
+/* raw device pointer and size of the CLA pool (for peer copies / profiling) */
+int gb_get_partials_pool(int instance, void **devicePtr, long long *bytes);
+/* out[0..4] = tipCount, partialsBufferCount, stateCount, categoryCount, patternCount */
+int gb_get_instance_shape(int instance, int *out);
+/* number of engine kernels launched since the instance was created */
+long long gb_get_launch_count(int instance);
+int gb_synchronize(int instance);
+/* message of the last failing call on this thread */
+const char *gb_last_error(void);
+/* instrumentation: the instance's CUDA stream (cudaStream_t) and optional
+ * CUDA-event timing of the CLA and edge kernels on that stream;
+ * timing out[0..4] = CLA ms, CLA launches, pattern-updates, edge ms, edge evaluations */
+int gb_get_stream(int instance, void **stream);
+int gb_set_kernel_timing(int instance, int on);
+int gb_get_kernel_timing(int instance, double *out);
+
+/* ---- host model math (model.cpp), used by the tree layer and by callers ---- */
+/* Model::UpdateQMat GTR branch (model.cpp:256-293) */
+int gbm_gtr_qmat(const double *rel6, const double *pi4, double *Q, double *blenMult);
+/* Model::UpdateQMatAminoAcid, estimated exchangeabilities (model.cpp:735-779) */
+int gbm_aa_qmat(const double *exch190, const double *pi20, double *Q, double *blenMult);
+/* Model::FillQMatLookup + UpdateQMatCodon, GY94 (model.cpp:296-687) */
+int gbm_codon_qmat(double kappa, double omega, const double *pi61, double *Q, double *blenMult);
+/* the same with six nucleotide-pair rates (AC, AG, AT, CG, CT, GT; nst = 6) */
+int gbm_codon_qmat6(const double *rel6, double omega, const double *pi61, double *Q, double *blenMult);
+/* Model::CalcEigenStuff (model.cpp:827-856) for a reversible Q */
+int gbm_eigen(int stateCount, const double *Q, const double *pi, double *eigenValues,
+              double *eigenVectors, double *inverseEigenVectors);
+/* Model::DiscreteGamma (model.cpp:2170-2201), mean-of-category rates */
+int gbm_discrete_gamma(double alpha, int categoryCount, double *rates);
+
+/* ---- tree layer: CalculationManager + Tree::Score / branch optimisation ----
+ * A C++ restatement of GARLI's holder bookkeeping (clamanager.h, treenode
+ * claIndexDown/UL/UR), dependency-levelled operation assembly
+ * (CalculationManager::DetermineRequiredOperations, calculationmanager.cpp:522-670)
+ * and the Newton-Raphson branch optimiser (optimization.cpp:1359-1971) on top
+ * of the instance API above.  Node numbering is GARLI's: 0 = trifurcating
+ * root, 1..ntax tips, ntax+1..2*ntax-3 internal; child3 = (left, middle|-1,
+ * right) per node. */
+int gbt_create(int instance, int ntax, const int *child3, const double *dlen);
+int gbt_destroy(int tree);
+/* model of the tree: eigen system (unscaled eigenvalues), blen multiplier,
+ * frequencies, category rates/weights and pinv */
+int gbt_set_model(int tree, const double *eigenValues, const double *eigenVectors,
+                  const double *inverseEigenVectors, double blenMult, const double *pi,
+                  const double *rates, const double *weights, double pinv, int hasPinv);
+/* Tree::Score (tree.cpp:4003) with the rescale retry loop; out[0] = lnL */
+int gbt_score(int tree, int rootNode, double *out);
+/* Tree::CalcDerivativesRateHet(nd->anc, nd) (optimization.cpp:1099): out = lnL, d1, d2 */
+int gbt_derivatives(int tree, int node, double *out);
+/* Tree::SetBranchLength + SweepDirtynessOverTree (tree.cpp:4247) */
+int gbt_set_branch_length(int tree, int node, double length);
+int gbt_get_branch_lengths(int tree, double *dlen);
+/* Tree::MakeAllNodesDirty */
+int gbt_make_all_dirty(int tree);
+/* NewtonRaphsonOptimizeBranchLength (optimization.cpp:1359); out[0] = estimated improvement */
+int gbt_optimize_branch(int tree, double precision, int node, double *out);
+/* OptimizeAllBranches (optimization.cpp:97); out[0] = improvement, out[1] = final lnL */
+int gbt_optimize_all_branches(int tree, double precision, double *out);
+int gbt_get_rescale_every(int tree);
+int gbt_set_rescale_every(int tree, int every);
+/* counters: [0] CLA ops issued, [1] pattern-updates (ops x patterns),
+ * [2] edge evaluations, [3] scores, [4] rescale retries */
+int gbt_get_counters(int tree, long long *out5);
+/* CLA buffer index currently holding (node, which) with which 0=Down 1=UL 2=UR; -1 if dirty */
+int gbt_cla_buffer(int tree, int node, int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GARLI_B200_H */

@@ -1,0 +1,61 @@
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+def load_fixture(name):
+    """Golden fixture written by tests/golden/make_fixtures.py."""
+    from garli_b200.patterns import PatternData
+
+    with open(os.path.join(GOLDEN, name)) as f:
+        fx = json.load(f)
+    tips = np.array([list(bytes.fromhex(h)) for h in fx["tips_hex"]], dtype=np.uint8)
+    pd = PatternData(fx["nstates"], tips, np.array(fx["counts"], dtype=np.int32), fx["last_const"],
+                     np.array(fx["const_states"], dtype=np.int32), fx["nsites"])
+    return fx, pd, np.array(fx["child3"], dtype=np.int32), np.array(fx["dlen"], dtype=np.float64)
+
+
+def fixture_model(fx, mathlib):
+    """Model of a fixture, built with ``mathlib``'s Q/eigen/gamma (oracle or engine)."""
+    from garli_b200.engine import Model
+
+    m = fx["model"]
+    if fx["nstates"] == 4:
+        pi = np.array(m["e"], dtype=np.float64)
+        pi = pi / pi.sum()
+        Q, bm = mathlib.gtr_qmat(m["r"], pi)
+        rates = mathlib.discrete_gamma(m["a"], m["ncat"])
+        pinv = m["p"]
+        has = True
+    else:
+        pi = np.array(m["e_empirical"], dtype=np.float64)
+        Q, bm = mathlib.codon_qmat6(m["r"], m["o"][0], pi)
+        rates = np.ones(1)
+        pinv, has = 0.0, False
+    ev, U, Ui = mathlib.eigen(Q, pi)
+    R = len(rates)
+    return Model(fx["nstates"], pi, Q, bm, ev, U, Ui, np.asarray(rates, dtype=np.float64),
+                 np.full(R, (1.0 - pinv) / R), pinv, has)
+
+
+@pytest.fixture(scope="session")
+def has_gpu():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False

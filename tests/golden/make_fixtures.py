@@ -1,0 +1,169 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own test data.
+
+Reads, from the reference tree (never at test time):
+  garli/trunk/tests/data/z.11x2178.nex     11 taxa x 2,178 sites (DNA)
+  garli/trunk/tests/data/n.G4.start        GTR+I+G4 start tree + [!GarliScore] + [!GarliModel]
+  garli/trunk/tests/data/n.G5.start        GTR+I+G5
+  garli/trunk/tests/data/c.start           codon (6 nucleotide rates, one omega class)
+
+and writes JSON fixtures holding the compressed site patterns (GARLI's
+PatternManager order, garli_b200/patterns.py), the tree in GARLI's node layout,
+the model parameters printed by GARLI and GARLI's own score for that tree.
+The GarliScore comments are the pins: GARLI computed them with its CPU path
+before printing the parameters to 5 decimals, so a rescore agrees to about 1e-3.
+
+    python tests/golden/make_fixtures.py [/path/to/garli/trunk]
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from garli_b200 import patterns, treeio  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/garli/trunk"
+DATA = os.path.join(REF, "tests", "data")
+
+
+def read_nexus_matrix(path):
+    txt = open(path).read()
+    txt = re.sub(r"\[[^\]]*\]", "", txt)
+    m = re.search(r"matrix(.*?);", txt, re.S | re.I)
+    rows = {}
+    order = []
+    for line in m.group(1).strip().splitlines():
+        parts = line.split()
+        if len(parts) < 2:
+            continue
+        name, seq = parts[0], "".join(parts[1:])
+        if name not in rows:
+            order.append(name)
+            rows[name] = ""
+        rows[name] += seq
+    return order, rows
+
+
+def read_start(path):
+    txt = open(path).read()
+    block = re.search(r"translate(.*?);", txt, re.S | re.I).group(1)
+    trans = dict((num, name) for num, name in re.findall(r"(\d+)\s+([^\s,;]+)", block))
+    score = float(re.search(r"GarliScore\s+([-0-9.]+)", txt).group(1))
+    model = re.search(r"GarliModel([^\]]*)\]", txt).group(1).split()
+    newick = re.search(r"tree\s+\S+\s*=\s*(.*?;)", txt, re.S).group(1)
+    params = {}
+    key = None
+    for tok in model:
+        if re.fullmatch(r"[a-z]", tok):
+            key = tok
+            params[key] = []
+        else:
+            params[key].append(float(tok))
+    return trans, score, params, newick
+
+
+def dna_fixture(start_name, ncat):
+    order, rows = read_nexus_matrix(os.path.join(DATA, "z.11x2178.nex"))
+    trans, score, params, newick = read_start(os.path.join(DATA, start_name))
+    num_of = {name: int(num) for num, name in trans.items()}
+    ntax = len(order)
+    masks = np.zeros((ntax, len(rows[order[0]])), dtype=np.uint8)
+    for name in order:
+        masks[num_of[name] - 1] = [patterns.DNA_CODES[c.upper()] for c in rows[name]]
+    pd = patterns.compress(masks, 4)
+    tree = treeio.parse_newick(newick)
+    child3, dlen = treeio.to_garli(tree)
+    return {
+        "source": f"garli/trunk/tests/data/z.11x2178.nex + {start_name}",
+        "nstates": 4,
+        "ntax": ntax,
+        "nsites": int(pd.nsites),
+        "npat": int(pd.npat),
+        "tips_hex": [bytes(r.tolist()).hex() for r in pd.tips],
+        "counts": pd.counts.tolist(),
+        "last_const": int(pd.last_const),
+        "const_states": pd.const_states.tolist(),
+        "child3": child3.tolist(),
+        "dlen": dlen.tolist(),
+        "model": {"r": params["r"], "e": params["e"], "a": params.get("a", [None])[0],
+                  "p": params.get("p", [0.0])[0], "ncat": ncat},
+        "garli_score": score,
+    }
+
+
+STD_CODE = "KNKNTTTTRSRSIIMIQHQHPPPPRRRRLLLLEDEDAAAAGGGGVVVV*Y*YSSSS*CWCLFLF"
+
+
+def codon_fixture(start_name):
+    """CodonData::FillCodonMatrixFromDNA (sequencedata.cpp:364-440): ACGT base-4
+    codon numbering, stop codons removed, any gap or ambiguity -> missing (61)."""
+    order, rows = read_nexus_matrix(os.path.join(DATA, "z.11x2178.nex"))
+    trans, score, params, newick = read_start(os.path.join(DATA, start_name))
+    num_of = {name: int(num) for num, name in trans.items()}
+    ntax = len(order)
+    sense = [c for c in range(64) if STD_CODE[c] != "*"]
+    index_of = {c: i for i, c in enumerate(sense)}
+    idx = {"A": 0, "C": 1, "G": 2, "T": 3, "U": 3}
+    ncod = len(rows[order[0]]) // 3
+    states = np.zeros((ntax, ncod), dtype=np.uint8)
+    for name in order:
+        s = rows[name].upper()
+        out = []
+        for k in range(ncod):
+            trip = s[3 * k: 3 * k + 3]
+            if all(ch in idx for ch in trip):
+                c = idx[trip[0]] * 16 + idx[trip[1]] * 4 + idx[trip[2]]
+                out.append(index_of[c])
+            else:
+                out.append(61)
+        states[num_of[name] - 1] = out
+    pd = patterns.compress(states, 61)
+    # CodonData::CalcEmpiricalFreqs, CODON_TABLE (sequencedata.cpp:228-276): observed
+    # codon counts over all taxa and patterns, one pseudo-count each if any is zero
+    emp = np.zeros(61)
+    for t in range(ntax):
+        for j in range(pd.npat):
+            if pd.tips[t, j] != 61:
+                emp[pd.tips[t, j]] += pd.counts[j]
+    if (emp == 0).any():
+        emp += 1.0
+    emp = emp / emp.sum()
+    tree = treeio.parse_newick(newick)
+    child3, dlen = treeio.to_garli(tree)
+    return {
+        "source": f"garli/trunk/tests/data/z.11x2178.nex (as codons) + {start_name}",
+        "nstates": 61,
+        "ntax": ntax,
+        "nsites": int(pd.nsites),
+        "npat": int(pd.npat),
+        "tips_hex": [bytes(r.tolist()).hex() for r in pd.tips],
+        "counts": pd.counts.tolist(),
+        "last_const": int(pd.last_const),
+        "const_states": pd.const_states.tolist(),
+        "child3": child3.tolist(),
+        "dlen": dlen.tolist(),
+        "model": {"r": params["r"], "e": params["e"], "e_empirical": emp.tolist(), "o": params["o"], "ncat": 1},
+        "garli_score": score,
+    }
+
+
+def main():
+    out = {
+        "z11x2178_nG4.json": dna_fixture("n.G4.start", 4),
+        "z11x2178_nG5.json": dna_fixture("n.G5.start", 5),
+        "z11x2178_codon.json": codon_fixture("c.start"),
+    }
+    for name, obj in out.items():
+        with open(os.path.join(HERE, name), "w") as f:
+            json.dump(obj, f, separators=(",", ":"))
+        print(name, obj["npat"], "patterns, GarliScore", obj["garli_score"])
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,205 @@
+"""Parity of the CUDA engine with the CPU oracle, through the C ABI (needs a B200).
+
+Tolerances:
+  * plain FP64 form: lnL, d1, d2 to 1e-8 relative (|dlnL| <= 1e-8 |lnL|); CLA
+    entries to 1e-12 (4 states) / 1e-9 (61 states) of each pattern's largest
+    entry (P(t) uses the device exp, which may differ from the host's by an
+    ulp); integer rescale counts and ranks exactly.
+  * precision form (FP32 CLAs, power-of-two scalers): |dlnL| <= 1e-4 * max(1, npat/2000)
+    absolute per tree, derivatives to 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import fixture_model, load_fixture
+from garli_b200 import engine, synth
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+PINS = ["z11x2178_nG4.json", "z11x2178_nG5.json", "z11x2178_codon.json"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    if engine.lib().gb_get_device_count() < 1:
+        pytest.fail("no CUDA device visible to the engine")
+
+
+def _both(pd, c3, dl, model, mixed=False):
+    inst, tree = engine.tree_engine(pd, c3, dl, model, mixed=mixed)
+    ot = orc.OracleTree(pd, c3, dl, model)
+    return inst, tree, ot
+
+
+@pytest.mark.parametrize("name", PINS)
+def test_fixture_scores_match_oracle_and_garli(name):
+    fx, pd, c3, dl = load_fixture(name)
+    m = fixture_model(fx, engine)
+    inst, tree, ot = _both(pd, c3, dl, m)
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
+    assert abs(lg - fx["garli_score"]) < 2e-6
+    assert np.allclose(inst.site_lnl(), ot.site_lnl(), rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("name", PINS)
+def test_every_cla_and_scaler_matches(name):
+    """After a full score from node 0 every clean CLA equals the oracle's; scalers exactly."""
+    fx, pd, c3, dl = load_fixture(name)
+    m = fixture_model(fx, engine)
+    inst, tree, ot = _both(pd, c3, dl, m)
+    for tr in (tree, ot):
+        tr.rescale_every = 2  # force rescaling on every eligible CLA
+        tr.score(0)
+    n = 0
+    for nd in [0] + list(range(pd.ntax + 1, c3.shape[0])):
+        for w in range(3):
+            b = tree.cla_buffer(nd, w)
+            arr, mult = ot.cla(nd, w)
+            assert (b >= 0) == (arr is not None)
+            if b < 0:
+                continue
+            g = inst.partials(b)
+            # normwise per pattern: 61-state P(t) sums cancel, so entries far below a
+            # pattern's largest carry the ulp-level exp differences of host vs device
+            tol = 1e-12 if pd.nstates == 4 else 1e-9
+            scale = np.abs(arr).max(axis=(1, 2), keepdims=True)
+            assert (np.abs(g - arr) <= tol * scale).all(), (nd, w, np.abs(g - arr).max())
+            assert np.array_equal(inst.scale_factors(b), mult)
+            assert engine.lib().gb_get_rescale_rank(inst.h, b) == ot.cla_rank(nd, w)
+            n += 1
+    assert n >= pd.ntax - 2
+
+
+@pytest.mark.parametrize("name", PINS)
+def test_branch_derivatives(name):
+    fx, pd, c3, dl = load_fixture(name)
+    m = fixture_model(fx, engine)
+    inst, tree, ot = _both(pd, c3, dl, m)
+    for nd in range(1, c3.shape[0]):
+        g = tree.derivatives(nd)
+        o = ot.derivatives(nd)
+        assert abs(g[0] - o[0]) <= 1e-8 * abs(o[0])
+        assert abs(g[1] - o[1]) <= 1e-8 * max(1.0, abs(o[1])), (nd, g, o)
+        assert abs(g[2] - o[2]) <= 1e-8 * max(1.0, abs(o[2])), (nd, g, o)
+
+
+def test_root_choice_and_rescale_invariance():
+    fx, pd, c3, dl = load_fixture(PINS[0])
+    m = fixture_model(fx, engine)
+    inst, tree, ot = _both(pd, c3, dl, m)
+    ref = ot.score(0)
+    for nd in [0] + list(range(pd.ntax + 1, c3.shape[0])):
+        tree.make_all_dirty()
+        assert abs(tree.score(nd) - ref) <= 1e-8 * abs(ref)
+    tree.rescale_every = 2
+    tree.make_all_dirty()
+    assert abs(tree.score(0) - ref) <= 1e-8 * abs(ref)
+
+
+def test_config0_score_and_newton_pass():
+    """32 taxa x 2,000 sites GTR+G4: full score plus one all-branch Newton pass."""
+    w = synth.dna_small()
+    inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model)
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
+    ig, fg = tree.optimize_all_branches(0.01)
+    io, fo = ot.optimize_all_branches(0.01)
+    assert abs(fg - fo) <= 1e-8 * abs(fo)
+    assert np.allclose(tree.branch_lengths(), ot.branch_lengths(), rtol=1e-6, atol=1e-10)
+    tree.make_all_dirty()
+    ot.make_all_dirty()
+    assert abs(tree.score(0) - ot.score(0)) <= 1e-8 * abs(lo)
+
+
+def _underflowing_case(seed=11, ntax=96, nsites=300, blen=1e-5):
+    """Random tip states on short branches: every site needs many substitutions, so
+    site likelihoods fall by ~1e-3 per mismatch and cross 1e-190 within one
+    rescale window unless rescaleEvery is small."""
+    from garli_b200.patterns import compress
+
+    rng = np.random.default_rng(seed)
+    c3, dl = synth.yule_tree(ntax, rng, 0.1)
+    dl[:] = blen
+    dl[0] = 0.0
+    m = synth.gtr_model(rng)
+    states = rng.integers(4, size=(ntax, nsites))
+    return c3, dl, m, compress(synth.dna_to_masks(states), 4)
+
+
+def test_rescale_retry_path_matches_oracle():
+    """GARLI's throw(1) -> rescaleEvery -= 2 retry (tree.cpp:3442, :4077)."""
+    c3, dl, m, pd = _underflowing_case()
+    inst, tree, ot = _both(pd, c3, dl, m)
+    for tr in (tree, ot):
+        tr.rescale_every = 160
+    lo = ot.score(0)
+    lg = tree.score(0)
+    assert ot.rescale_every < 160, "case did not trigger the retry path"
+    assert tree.rescale_every == ot.rescale_every
+    assert tree.counters()["rescale_retries"] == (160 - ot.rescale_every) // 2
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
+
+
+@pytest.mark.parametrize("kind", ["aa", "codon"])
+def test_nstate_synthetic(kind):
+    w = synth.aa(seed=4, ntax=16, nsites=600) if kind == "aa" else synth.codon(seed=5, ntax=12, ncodons=300)
+    inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model)
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
+    for nd in (1, 5, w.data.ntax + 2):
+        g, o = tree.derivatives(nd), ot.derivatives(nd)
+        assert np.allclose(g, o, rtol=1e-8, atol=1e-8)
+
+
+@pytest.mark.parametrize("name", PINS)
+def test_mixed_precision_form(name):
+    fx, pd, c3, dl = load_fixture(name)
+    m = fixture_model(fx, engine)
+    inst, tree = engine.tree_engine(pd, c3, dl, m, mixed=True)
+    ot = orc.OracleTree(pd, c3, dl, m)
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-4 * max(1.0, pd.npat / 2000)
+    for nd in (1, 4, pd.ntax + 3):
+        g, o = tree.derivatives(nd), ot.derivatives(nd)
+        assert abs(g[0] - o[0]) <= 1e-4 * max(1.0, pd.npat / 2000)
+        assert abs(g[1] - o[1]) <= 1e-4 * max(1.0, abs(o[1]))
+        assert abs(g[2] - o[2]) <= 1e-4 * max(1.0, abs(o[2]))
+
+
+def test_abi_operation_lists_directly():
+    """Drive the instance ABI with hand-built ClaOperation lists (tip-tip, int-tip, int-int)."""
+    w = synth.make_dna(6, 400, seed=3)
+    pd, c3, dl, m = w.data, w.child3, w.dlen, w.model
+    ntip = 6
+    inst = engine.Instance(ntip, 12, 4, pd.npat, 4, 10)
+    inst.set_data(pd)
+    inst.set_model(m)
+    inst.update_transition_matrices([(i, dl[i], 0, 1) for i in range(1, 10)])
+    ot = orc.OracleTree(pd, c3, dl, m)
+    lo = ot.score(0)
+
+    def buf(nd):  # tips 1..6 -> 0..5; internal 0, 7, 8, 9 -> 6..9
+        return nd - 1 if 1 <= nd <= ntip else ntip + (0 if nd == 0 else nd - ntip)
+
+    level = {}
+    ops = []
+
+    def post(nd):
+        l, r = int(c3[nd][0]), int(c3[nd][2])
+        if nd == 0 and c3[0][1] > ntip:
+            post(int(c3[0][1]))
+        for k in (l, r):
+            if k > ntip:
+                post(k)
+        lvl = 1 + max([level[k] for k in (l, r) if k > ntip] or [0])
+        level[nd] = lvl
+        ops.append((buf(nd), buf(l), buf(r), l, r, lvl))
+
+    post(0)
+    inst.update_partials(ops, 16)
+    mid = int(c3[0][1])
+    out = inst.calculate_edge(buf(0), buf(mid), mid, derivatives=False)
+    assert abs(out[0] - lo) <= 1e-8 * abs(lo)
+    assert inst.launch_count() > 0

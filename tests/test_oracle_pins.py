@@ -1,0 +1,126 @@
+"""The CPU oracle against the reference's own pins and invariants (no GPU).
+
+Pins: GARLI's [!GarliScore] of the start trees in garli/trunk/tests/data
+(n.G4.start, n.G5.start, c.start), recomputed from the parameters GARLI printed
+with them.  Invariants: Population::RunTests (population.cpp:845-966).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import fixture_model, load_fixture
+from oracle import oracle as orc
+
+PINS = ["z11x2178_nG4.json", "z11x2178_nG5.json", "z11x2178_codon.json"]
+
+
+@pytest.mark.parametrize("name", PINS)
+def test_oracle_reproduces_garli_score(name):
+    fx, pd, c3, dl = load_fixture(name)
+    t = orc.OracleTree(pd, c3, dl, fixture_model(fx, orc))
+    lnl = t.score(0)
+    # GARLI prints the score with 6 decimals; the restated path agrees to < 1e-6
+    assert abs(lnl - fx["garli_score"]) < 2e-6, (lnl, fx["garli_score"])
+
+
+@pytest.mark.parametrize("name", PINS[:2])
+def test_root_invariance(name):
+    """Minimal-recalc scores from every internal node agree (population.cpp:924-954)."""
+    fx, pd, c3, dl = load_fixture(name)
+    t = orc.OracleTree(pd, c3, dl, fixture_model(fx, orc))
+    ref = t.score(0)
+    for nd in [0] + list(range(pd.ntax + 1, c3.shape[0])):
+        t.make_all_dirty()
+        assert abs(t.score(nd) - ref) < 1e-9 * abs(ref)
+
+
+def test_rescale_frequency_invariance():
+    """rescaleEvery = 2 scores the same as the default 16 (population.cpp:896-908)."""
+    fx, pd, c3, dl = load_fixture(PINS[0])
+    t = orc.OracleTree(pd, c3, dl, fixture_model(fx, orc))
+    ref = t.score(0)
+    t.rescale_every = 2
+    t.make_all_dirty()
+    assert abs(t.score(0) - ref) < 1e-9 * abs(ref)
+
+
+def test_derivative_lnl_equals_score():
+    """The lnL returned with the derivatives equals Score()'s (population.cpp:956-964)."""
+    fx, pd, c3, dl = load_fixture(PINS[0])
+    t = orc.OracleTree(pd, c3, dl, fixture_model(fx, orc))
+    ref = t.score(0)
+    for nd in range(1, c3.shape[0]):
+        d = t.derivatives(nd)
+        assert abs(d[0] - ref) < 1e-9 * abs(ref)
+
+
+def test_derivatives_match_finite_differences():
+    fx, pd, c3, dl = load_fixture(PINS[0])
+    t = orc.OracleTree(pd, c3, dl, fixture_model(fx, orc))
+    for nd in (3, 14, 17):
+        v = t.branch_lengths()[nd]
+        d = t.derivatives(nd)
+        h = 1e-5
+        t.set_branch_length(nd, v + h); lp = t.score(0)
+        t.set_branch_length(nd, v - h); lm = t.score(0)
+        t.set_branch_length(nd, v)
+        assert abs((lp - lm) / (2 * h) - d[1]) < 1e-4 * max(1.0, abs(d[1]))
+        assert abs((lp - 2 * t.score(0) + lm) / h**2 - d[2]) < 1e-2 * max(1.0, abs(d[2]))
+
+
+def test_branch_optimisation_does_not_worsen():
+    """OptimizeAllBranches never lowers lnL (population.cpp:892-894)."""
+    fx, pd, c3, dl = load_fixture(PINS[0])
+    t = orc.OracleTree(pd, c3, dl * 1.7, fixture_model(fx, orc))
+    before = t.score(0)
+    imp, after = t.optimize_all_branches(0.01)
+    t.make_all_dirty()
+    assert t.score(0) >= before - 1e-3
+    assert after >= before
+
+
+def test_rescale_tables_match_tree_cpp():
+    incr, thresh, mult = orc.rescale_tables()
+    assert incr[0] == 24 and incr[1] == 31 and incr[89] == 24 + 7 * 89
+    assert np.allclose(thresh, np.exp(-incr.astype(float)), rtol=1e-15, atol=0)
+    assert mult[0] == np.exp(24.0)
+    assert (mult <= 1e250).all()
+
+
+def test_discrete_gamma_matches_exact_quantiles():
+    sp = pytest.importorskip("scipy.special")
+    st = pytest.importorskip("scipy.stats")
+    for a, n in [(0.5, 4), (1.25046, 4), (1.34382, 5), (0.8, 4), (2.0, 8)]:
+        q = st.gamma.ppf(np.arange(1, n) / n, a, scale=1 / a)
+        cum = np.concatenate([[0.0], sp.gammainc(a + 1, q * a), [1.0]])
+        # the Stirling log-gamma (as in model.cpp LnGamma) bounds agreement at ~1e-10
+        assert np.allclose(orc.discrete_gamma(a, n), np.diff(cum) * n, rtol=1e-9, atol=1e-10)
+
+
+def test_oracle_and_engine_eigensystems_match_garli_linalg():
+    """Both eigensolvers give GARLI's EigenRealGeneral P(t) (oracle/_ref, built from linalg.cpp)."""
+    so = os.path.join(os.path.dirname(orc.__file__), "_ref", "libref_linalg.so")
+    if not os.path.exists(so):
+        pytest.skip("oracle/_ref not built (needs the reference sources)")
+    import ctypes as C
+
+    from garli_b200 import synth
+
+    L = C.CDLL(so)
+    D = C.POINTER(C.c_double)
+    L.ref_eigen.argtypes = [C.c_int, D, D, D, D]
+    rng = np.random.default_rng(0)
+    for mk in (synth.gtr_model, synth.aa_model, synth.codon_model):
+        m = mk(rng)
+        n = m.nstates
+        ev, U, Ui = np.zeros(n), np.zeros((n, n)), np.zeros((n, n))
+        Q = np.ascontiguousarray(m.Q)
+        assert L.ref_eigen(n, Q.ctypes.data_as(D), ev.ctypes.data_as(D), U.ctypes.data_as(D), Ui.ctypes.data_as(D)) == 0
+        for t in (0.01, 0.3, 2.0):
+            Pref = U @ np.diag(np.exp(ev * m.blen_mult * t)) @ Ui
+            e2, U2, Ui2 = orc.eigen(m.Q, m.pi)
+            Po = U2 @ np.diag(np.exp(e2 * m.blen_mult * t)) @ Ui2
+            Pe = m.U @ np.diag(np.exp(m.eval * m.blen_mult * t)) @ m.Uinv
+            assert np.abs(Po - Pref).max() < 1e-13
+            assert np.abs(Pe - Pref).max() < 1e-13
