@@ -28,23 +28,39 @@ struct LevelOps {
 };
 
 // Device view of an instance, passed by value to every kernel.
+// A CLA buffer holds its first `kpad` patterns in FP64 and the rest in FP32
+// (kpad = all patterns in the plain form; in the precision form the patterns
+// with large counts, placed first by the instance's internal permutation).
 struct View {
-    void *partials;           // nbuf x cla_stride elements (double or float)
+    char *partials;           // nbuf x cla_bytes
     int *scalers;             // nbuf x npat_pad
     const uint8_t *tips;      // ntip x npat_pad
     const double *mats;       // nmat x mat_stride: [P | dP | d2P], each R*S*S
     const int *counts;        // npat_pad (0 in the padding)
-    const int *const_states;  // npat_pad
+    const int *const_states;  // npat_pad; -1 = not a constant pattern
     const double *freqs;      // S
     const double *rate_probs; // R
     int *status;
     double *block_sums;       // kMaxScoreBlocks x 3
     double *site_lnl;         // npat_pad
-    long long cla_stride;     // elements per CLA buffer = npat_pad * R * S
+    long long cla_bytes;      // bytes per CLA buffer
     long long mat_stride;     // 3 * R * S * S
-    int npat, npat_pad, ntip, last_const, has_pinv, rescale_every;
+    int npat, npat_pad, ntip, kpad, has_pinv, rescale_every;
     double pinv;
 };
+
+// Pointer to the R*S slice of pattern p in CLA buffer b (ST must match p's segment).
+template <typename ST>
+__device__ __forceinline__ ST *cla_ptr(const View &v, int b, int p, int RS);
+template <>
+__device__ __forceinline__ double *cla_ptr<double>(const View &v, int b, int p, int RS) {
+    return reinterpret_cast<double *>(v.partials + (long long)b * v.cla_bytes) + (long long)p * RS;
+}
+template <>
+__device__ __forceinline__ float *cla_ptr<float>(const View &v, int b, int p, int RS) {
+    return reinterpret_cast<float *>(v.partials + (long long)b * v.cla_bytes + (long long)v.kpad * RS * 8) +
+           (long long)(p - v.kpad) * RS;
+}
 
 // rescale tables (tree.cpp:163-172), filled from the host with the same libm
 // (defined here: the engine is a single CUDA translation unit)

@@ -78,34 +78,19 @@ __device__ __forceinline__ void tip_vec(const double *P, int c, double tv[4]) {
 //   Tree::RescaleRateHet                tree.cpp:3370 (plain form, rank-gated)
 // ---------------------------------------------------------------------------
 template <typename ST, int R, bool GARLI_SCALE>
-__global__ void __launch_bounds__(kThreads) k_cla4(View v, LevelOps ops) {
+__device__ __forceinline__ void cla4_body(const View &v, const DevOp &op, const double *PL, const double *PR, int tile) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
-    const DevOp op = ops.op[blockIdx.y];
-    __shared__ double sP[2][R * 16];
-    {
-        const double *m1 = v.mats + (long long)op.p1 * v.mat_stride;
-        const double *m2 = v.mats + (long long)op.p2 * v.mat_stride;
-        for (int i = threadIdx.x; i < R * 16; i += blockDim.x) {
-            sP[0][i] = m1[i];
-            sP[1][i] = m2[i];
-        }
-    }
-    __syncthreads();
     const int r = threadIdx.x % G;
-    const int p = blockIdx.x * PPB + threadIdx.x / G;
+    const int p = tile * PPB + threadIdx.x / G;
     const bool act = (p < v.npat) && (r < R);
-    ST *base = reinterpret_cast<ST *>(v.partials);
     double d[4] = {0.0, 0.0, 0.0, 0.0};
     int m = 0;
-    const long long off = (long long)p * (R * 4) + r * 4;
     if (act) {
-        const double *PL = &sP[0][16 * r];
-        const double *PR = &sP[1][16 * r];
         if (op.kind == kIntInt) {
             double a[4], b[4];
-            cla_load<ST>(base + (long long)op.c1 * v.cla_stride + off, a);
-            cla_load<ST>(base + (long long)op.c2 * v.cla_stride + off, b);
+            cla_load<ST>(cla_ptr<ST>(v, op.c1, p, R * 4) + r * 4, a);
+            cla_load<ST>(cla_ptr<ST>(v, op.c2, p, R * 4) + r * 4, b);
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 double L = (R == 4) ? dot4_pair(PL + 4 * i, a) : dot4_seq(PL + 4 * i, a);
@@ -115,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) k_cla4(View v, LevelOps ops) {
             if (r == 0) m = v.scalers[(long long)op.c1 * v.npat_pad + p] + v.scalers[(long long)op.c2 * v.npat_pad + p];
         } else if (op.kind == kIntTip) {
             double a[4];
-            cla_load<ST>(base + (long long)op.c1 * v.cla_stride + off, a);
+            cla_load<ST>(cla_ptr<ST>(v, op.c1, p, R * 4) + r * 4, a);
             const int code = v.tips[(long long)op.c2 * v.npat_pad + p];
             const int cls = tip_class(code);
             if (cls == 0) {
@@ -123,7 +108,9 @@ __global__ void __launch_bounds__(kThreads) k_cla4(View v, LevelOps ops) {
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     double L = (R == 4) ? dot4_pair(PL + 4 * i, a) : dot4_seq(PL + 4 * i, a);
-                    d[i] = mul(L, PR[4 * i + s]);
+                    // register-resident P: select column s without dynamic indexing
+                    const double pr = s == 0 ? PR[4 * i] : s == 1 ? PR[4 * i + 1] : s == 2 ? PR[4 * i + 2] : PR[4 * i + 3];
+                    d[i] = mul(L, pr);
                 }
             } else if (cls == 1) {
 #pragma unroll
@@ -173,8 +160,36 @@ __global__ void __launch_bounds__(kThreads) k_cla4(View v, LevelOps ops) {
         }
     }
     if (act) {
-        cla_store<ST>(base + (long long)op.dest * v.cla_stride + off, d);
+        cla_store<ST>(cla_ptr<ST>(v, op.dest, p, R * 4) + r * 4, d);
         if (r == 0) v.scalers[(long long)op.dest * v.npat_pad + p] = m;
+    }
+}
+
+// P(t) of this lane's rate category for both children stay in registers; the
+// block walks its share of pattern tiles (grid-stride), so the per-block setup
+// is amortised over many tiles.
+template <int R, bool GARLI_SCALE>
+__global__ void __launch_bounds__(kThreads) k_cla4(View v, LevelOps ops) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    const DevOp op = ops.op[blockIdx.y];
+    const int r = threadIdx.x % G;
+    const int rr = r < R ? r : 0;
+    double PL[16], PR[16];
+    {
+        const double *m1 = v.mats + (long long)op.p1 * v.mat_stride + 16 * rr;
+        const double *m2 = v.mats + (long long)op.p2 * v.mat_stride + 16 * rr;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            PL[i] = __ldg(m1 + i);
+            PR[i] = __ldg(m2 + i);
+        }
+    }
+    const int ntiles = (v.npat + PPB - 1) / PPB;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // kpad is a multiple of 128, so a tile never straddles the FP64/FP32 boundary
+        if (tile * PPB < v.kpad) cla4_body<double, R, GARLI_SCALE>(v, op, PL, PR, tile);
+        else cla4_body<float, R, GARLI_SCALE>(v, op, PL, PR, tile);
     }
 }
 
@@ -216,126 +231,140 @@ __device__ __forceinline__ void block_sum3(double a, double b, double c, double 
 //   Tree::GetDerivsPartialTerminal        optimization.cpp:2412
 // One thread per pattern; the rate loop runs in the reference's order.
 // ---------------------------------------------------------------------------
+template <int R, bool DERIV>
+struct EdgeSmem {
+    double M[3][R * 16];
+    double F[4], RP[R];
+};
+
 template <typename ST, int R, bool GARLI_SCALE, bool DERIV>
-__global__ void __launch_bounds__(kThreads) k_edge4(View v, int pbuf, int cbuf, int mat, int child_tip,
-                                                    int write_sites) {
-    __shared__ double sM[3][R * 16];
-    __shared__ double sF[4], sRP[R];
-    {
-        const double *mp = v.mats + (long long)mat * v.mat_stride;
-        for (int i = threadIdx.x; i < R * 16; i += blockDim.x) {
-            sM[0][i] = mp[i];
-            if (DERIV) {
-                sM[1][i] = mp[R * 16 + i];
-                sM[2][i] = mp[2 * R * 16 + i];
-            }
-        }
-        if (threadIdx.x < 4) sF[threadIdx.x] = v.freqs[threadIdx.x];
-        if (threadIdx.x < R) sRP[threadIdx.x] = v.rate_probs[threadIdx.x];
-    }
-    __syncthreads();
-    const ST *base = reinterpret_cast<const ST *>(v.partials);
-    const ST *PC = base + (long long)pbuf * v.cla_stride;
-    const ST *CC = child_tip ? nullptr : base + (long long)cbuf * v.cla_stride;
-    const int *pm = v.scalers + (long long)pbuf * v.npat_pad;
-    const int *cm = child_tip ? nullptr : v.scalers + (long long)cbuf * v.npat_pad;
-    const uint8_t *tip = child_tip ? v.tips + (long long)cbuf * v.npat_pad : nullptr;
-    const double *f = sF;
-    double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < v.npat; p += gridDim.x * blockDim.x) {
-        double L[4] = {0, 0, 0, 0}, D1[4] = {0, 0, 0, 0}, D2[4] = {0, 0, 0, 0};
-        const int m1 = pm[p];
-        const int m2 = child_tip ? 0 : cm[p];
-        if (!child_tip) {
+__device__ __forceinline__ void edge4_site(const View &v, const EdgeSmem<R, DERIV> &sm, int pbuf, int cbuf,
+                                           int child_tip, int write_sites, int p, double &accL, double &acc1,
+                                           double &acc2) {
+    const double *f = sm.F;
+    double L[4] = {0, 0, 0, 0}, D1[4] = {0, 0, 0, 0}, D2[4] = {0, 0, 0, 0};
+    const int m1 = v.scalers[(long long)pbuf * v.npat_pad + p];
+    const int m2 = child_tip ? 0 : v.scalers[(long long)cbuf * v.npat_pad + p];
+    const ST *PC = cla_ptr<ST>(v, pbuf, p, R * 4);
+    if (!child_tip) {
+        const ST *CC = cla_ptr<ST>(v, cbuf, p, R * 4);
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                double part[4], c[4];
-                cla_load<ST>(PC + (long long)p * (R * 4) + r * 4, part);
-                cla_load<ST>(CC + (long long)p * (R * 4) + r * 4, c);
-                const double rp = sRP[r];
+        for (int r = 0; r < R; r++) {
+            double part[4], c[4];
+            cla_load<ST>(PC + r * 4, part);
+            cla_load<ST>(CC + r * 4, c);
+            const double rp = sm.RP[r];
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    L[i] = add(L[i], mul(mul(dot4_seq(&sM[0][16 * r + 4 * i], c), part[i]), rp));
-                    if (DERIV) {
-                        D1[i] = add(D1[i], mul(mul(dot4_seq(&sM[1][16 * r + 4 * i], c), part[i]), rp));
-                        D2[i] = add(D2[i], mul(mul(dot4_seq(&sM[2][16 * r + 4 * i], c), part[i]), rp));
-                    }
+            for (int i = 0; i < 4; i++) {
+                L[i] = add(L[i], mul(mul(dot4_seq(&sm.M[0][16 * r + 4 * i], c), part[i]), rp));
+                if (DERIV) {
+                    D1[i] = add(D1[i], mul(mul(dot4_seq(&sm.M[1][16 * r + 4 * i], c), part[i]), rp));
+                    D2[i] = add(D2[i], mul(mul(dot4_seq(&sm.M[2][16 * r + 4 * i], c), part[i]), rp));
                 }
             }
+        }
+    } else {
+        const int code = v.tips[(long long)cbuf * v.npat_pad + p] & 15;
+        const int cls = tip_class(code);
+        if (cls == 1) {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                double part[4];
+                cla_load<ST>(PC + r * 4, part);
+#pragma unroll
+                for (int i = 0; i < 4; i++) L[i] = add(L[i], mul(part[i], sm.RP[r]));
+            }
         } else {
-            const int code = tip[p] & 15;
-            const int cls = tip_class(code);
-            if (cls == 1) {
+            // single state: one pass; partial ambiguity: states outer, rates inner
+            for (int s = 0; s < 4; s++) {
+                if (!(code & (1 << s))) continue;
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     double part[4];
-                    cla_load<ST>(PC + (long long)p * (R * 4) + r * 4, part);
+                    cla_load<ST>(PC + r * 4, part);
+                    const double rp = sm.RP[r];
 #pragma unroll
-                    for (int i = 0; i < 4; i++) L[i] = add(L[i], mul(part[i], sRP[r]));
-                }
-            } else {
-                // single state: one pass; partial ambiguity: states outer, rates inner
-                for (int s = 0; s < 4; s++) {
-                    if (!(code & (1 << s))) continue;
-#pragma unroll
-                    for (int r = 0; r < R; r++) {
-                        double part[4];
-                        cla_load<ST>(PC + (long long)p * (R * 4) + r * 4, part);
-                        const double rp = sRP[r];
-#pragma unroll
-                        for (int i = 0; i < 4; i++) {
-                            L[i] = add(L[i], mul(mul(sM[0][16 * r + 4 * i + s], part[i]), rp));
-                            if (DERIV) {
-                                D1[i] = add(D1[i], mul(mul(sM[1][16 * r + 4 * i + s], part[i]), rp));
-                                D2[i] = add(D2[i], mul(mul(sM[2][16 * r + 4 * i + s], part[i]), rp));
-                            }
+                    for (int i = 0; i < 4; i++) {
+                        L[i] = add(L[i], mul(mul(sm.M[0][16 * r + 4 * i + s], part[i]), rp));
+                        if (DERIV) {
+                            D1[i] = add(D1[i], mul(mul(sm.M[1][16 * r + 4 * i + s], part[i]), rp));
+                            D2[i] = add(D2[i], mul(mul(sm.M[2][16 * r + 4 * i + s], part[i]), rp));
                         }
                     }
                 }
             }
         }
-        double siteL = add(add(add(mul(L[0], f[0]), mul(L[1], f[1])), mul(L[2], f[2])), mul(L[3], f[3]));
-        if (v.has_pinv && p <= v.last_const) {
-            const int cb = v.const_states[p];
-            double btot = 0.0;
-            if (cb & 1) btot = add(btot, f[0]);
-            if (cb & 2) btot = add(btot, f[1]);
-            if (cb & 4) btot = add(btot, f[2]);
-            if (cb & 8) btot = add(btot, f[3]);
-            if (GARLI_SCALE) {
-                if (DERIV) {
-                    // (prI*btot)*exp(child + partial) (optimization.cpp:2540, :3166)
-                    const double e = child_tip ? exp((double)m1) : exp(add((double)m2, (double)m1));
-                    siteL = add(siteL, mul(mul(v.pinv, btot), e));
-                } else if (m1 + m2 == 0) {
-                    siteL = add(siteL, mul(v.pinv, btot));
-                } else {
-                    // prI*btot*exp(partial + child) (tree.cpp:6128, :6236)
-                    siteL = add(siteL, mul(mul(v.pinv, btot), exp(add((double)m1, (double)m2))));
-                }
-            } else {
-                siteL = add(siteL, ldexp(mul(v.pinv, btot), m1 + m2));
-            }
-        }
-        double u;
+    }
+    double siteL = add(add(add(mul(L[0], f[0]), mul(L[1], f[1])), mul(L[2], f[2])), mul(L[3], f[3]));
+    const int cb = v.const_states[p];
+    if (v.has_pinv && cb >= 0) {
+        double btot = 0.0;
+        if (cb & 1) btot = add(btot, f[0]);
+        if (cb & 2) btot = add(btot, f[1]);
+        if (cb & 4) btot = add(btot, f[2]);
+        if (cb & 8) btot = add(btot, f[3]);
         if (GARLI_SCALE) {
-            const double lg = log(siteL);
-            if (DERIV && !child_tip) u = sub(sub(lg, (double)m2), (double)m1);
-            else u = sub(sub(lg, (double)m1), (double)m2);
+            if (DERIV) {
+                // (prI*btot)*exp(child + partial) (optimization.cpp:2540, :3166)
+                const double e = child_tip ? exp((double)m1) : exp(add((double)m2, (double)m1));
+                siteL = add(siteL, mul(mul(v.pinv, btot), e));
+            } else if (m1 + m2 == 0) {
+                siteL = add(siteL, mul(v.pinv, btot));
+            } else {
+                // prI*btot*exp(partial + child) (tree.cpp:6128, :6236)
+                siteL = add(siteL, mul(mul(v.pinv, btot), exp(add((double)m1, (double)m2))));
+            }
         } else {
-            u = sub(log(siteL), (double)(m1 + m2) * 0.69314718055994530941723212145818);
+            siteL = add(siteL, ldexp(mul(v.pinv, btot), m1 + m2));
         }
-        const double cnt = (double)v.counts[p];
-        accL = add(accL, mul(cnt, u));
+    }
+    double u;
+    if (GARLI_SCALE) {
+        const double lg = log(siteL);
+        if (DERIV && !child_tip) u = sub(sub(lg, (double)m2), (double)m1);
+        else u = sub(sub(lg, (double)m1), (double)m2);
+    } else {
+        u = sub(log(siteL), (double)(m1 + m2) * 0.69314718055994530941723212145818);
+    }
+    const double cnt = (double)v.counts[p];
+    accL = add(accL, mul(cnt, u));
+    if (DERIV) {
+        const double sd1 = add(add(add(mul(D1[0], f[0]), mul(D1[1], f[1])), mul(D1[2], f[2])), mul(D1[3], f[3])) / siteL;
+        const double sd2 =
+            sub(add(add(add(mul(D2[0], f[0]), mul(D2[1], f[1])), mul(D2[2], f[2])), mul(D2[3], f[3])) / siteL,
+                mul(sd1, sd1));
+        acc1 = add(acc1, mul(cnt, sd1));
+        acc2 = add(acc2, mul(cnt, sd2));
+    }
+    if (write_sites) v.site_lnl[p] = u;
+}
+
+template <int R, bool DERIV>
+__device__ __forceinline__ void edge4_load_smem(const View &v, int mat, EdgeSmem<R, DERIV> &sm) {
+    const double *mp = v.mats + (long long)mat * v.mat_stride;
+    for (int i = threadIdx.x; i < R * 16; i += blockDim.x) {
+        sm.M[0][i] = mp[i];
         if (DERIV) {
-            const double sd1 = add(add(add(mul(D1[0], f[0]), mul(D1[1], f[1])), mul(D1[2], f[2])), mul(D1[3], f[3])) / siteL;
-            const double sd2 =
-                sub(add(add(add(mul(D2[0], f[0]), mul(D2[1], f[1])), mul(D2[2], f[2])), mul(D2[3], f[3])) / siteL,
-                    mul(sd1, sd1));
-            acc1 = add(acc1, mul(cnt, sd1));
-            acc2 = add(acc2, mul(cnt, sd2));
+            sm.M[1][i] = mp[R * 16 + i];
+            sm.M[2][i] = mp[2 * R * 16 + i];
         }
-        if (write_sites) v.site_lnl[p] = u;
+    }
+    if (threadIdx.x < 4) sm.F[threadIdx.x] = v.freqs[threadIdx.x];
+    if (threadIdx.x < R) sm.RP[threadIdx.x] = v.rate_probs[threadIdx.x];
+}
+
+template <int R, bool GARLI_SCALE, bool DERIV>
+__global__ void __launch_bounds__(kThreads) k_edge4(View v, int pbuf, int cbuf, int mat, int child_tip,
+                                                    int write_sites) {
+    __shared__ EdgeSmem<R, DERIV> sm;
+    edge4_load_smem<R, DERIV>(v, mat, sm);
+    __syncthreads();
+    double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < v.npat; p += gridDim.x * blockDim.x) {
+        if (p < v.kpad)
+            edge4_site<double, R, GARLI_SCALE, DERIV>(v, sm, pbuf, cbuf, child_tip, write_sites, p, accL, acc1, acc2);
+        else
+            edge4_site<float, R, GARLI_SCALE, DERIV>(v, sm, pbuf, cbuf, child_tip, write_sites, p, accL, acc1, acc2);
     }
     block_sum3(accL, acc1, acc2, v.block_sums + 3 * blockIdx.x);
 }

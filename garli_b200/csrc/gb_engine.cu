@@ -18,6 +18,8 @@
 #include "../../include/garli_b200.h"
 #include "gb_common.cuh"
 #include "gb_dna.cuh"
+#include "gb_graph.cuh"
+#include "gb_newton_dna.cuh"
 #include "gb_nstate.cuh"
 #include "gb_pmat.cuh"
 
@@ -30,7 +32,16 @@ struct Instance {
     int ntip = 0, nbuf = 0, S = 0, R = 0, npat = 0, npat_pad = 0, neigen = 0, nmat = 0;
     long flags = 0;
     bool mixed = false;
-    size_t elem = 8;
+    size_t elem = 8;     // storage bytes of the FP32/FP64 bulk segment
+    int kpad = 0;        // patterns [0, kpad) stored in FP64 (internal order)
+    int kpad_cap = 0;    // FP64 segment size the buffers are laid out for
+    int nsm = 148;       // multiprocessors of the device
+    long long cla_bytes = 0;
+    // host copies in the caller's pattern order and the internal permutation
+    // (precision form: patterns with count >= kHeavyCount first, stored in FP64)
+    std::vector<uint8_t> h_tips;
+    std::vector<int> h_counts, h_cs;
+    std::vector<int> perm;  // internal pattern q holds caller pattern perm[q]
     cudaStream_t stream = nullptr;
     // device memory
     void *d_partials = nullptr;
@@ -56,19 +67,31 @@ struct Instance {
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
     std::vector<long long> ev_updates;
-    double cla_ms = 0.0;
+    std::vector<double> ev_bytes;
+    double cla_ms = 0.0, cla_bytes_timed = 0.0;
     long long cla_launches_timed = 0, cla_updates_timed = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_edge;
     double edge_ms = 0.0;
     long long edge_timed = 0;
+    // graph-resident branch-optimisation pass
+    double *d_len = nullptr;   // branch length per matrix index (device copy)
+    NrSlot *d_slots = nullptr; // Newton state per matrix index
+    unsigned long long version = 1;  // bumped by every setter baked into a graph
+    unsigned long long graph_key = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_nodes = 0;
 
-    long long cla_stride() const { return (long long)npat_pad * R * S; }
     long long mat_stride() const { return 3LL * R * S * S; }
     long long eig_stride() const { return (long long)S + 2LL * S * S; }
 };
 
 static std::mutex g_mu;
 static std::vector<Instance *> g_inst;
+
+// precision form: a pattern with at least this count keeps FP64 CLAs (its
+// rounding error would be multiplied by the count in the lnL sum)
+constexpr int kHeavyCount = 16;
 
 static Instance *get(int h) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -97,7 +120,7 @@ static int check_launch(Instance *I) {
 
 static View make_view(Instance *I) {
     View v;
-    v.partials = I->d_partials;
+    v.partials = reinterpret_cast<char *>(I->d_partials);
     v.scalers = I->d_scalers;
     v.tips = I->d_tips;
     v.mats = I->d_mats;
@@ -108,12 +131,12 @@ static View make_view(Instance *I) {
     v.status = I->d_status;
     v.block_sums = I->d_block_sums;
     v.site_lnl = I->d_site_lnl;
-    v.cla_stride = I->cla_stride();
+    v.cla_bytes = I->cla_bytes;
     v.mat_stride = I->mat_stride();
     v.npat = I->npat;
     v.npat_pad = I->npat_pad;
     v.ntip = I->ntip;
-    v.last_const = I->last_const;
+    v.kpad = I->kpad;
     v.has_pinv = I->has_pinv;
     v.rescale_every = 16;
     v.pinv = I->pinv;
@@ -144,32 +167,32 @@ static int upload_rescale_tables() {
 // ---------------------------------------------------------------------------
 // kernel dispatch
 // ---------------------------------------------------------------------------
-template <typename ST, bool G>
+template <bool G>
 static void launch_cla4(int R, dim3 grid, cudaStream_t st, const View &v, const LevelOps &ops) {
     switch (R) {
-        case 1: k_cla4<ST, 1, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 2: k_cla4<ST, 2, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 3: k_cla4<ST, 3, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 4: k_cla4<ST, 4, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 5: k_cla4<ST, 5, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 6: k_cla4<ST, 6, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 7: k_cla4<ST, 7, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        default: k_cla4<ST, 8, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 1: k_cla4<1, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 2: k_cla4<2, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 3: k_cla4<3, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 4: k_cla4<4, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 5: k_cla4<5, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 6: k_cla4<6, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        case 7: k_cla4<7, G><<<grid, kThreads, 0, st>>>(v, ops); break;
+        default: k_cla4<8, G><<<grid, kThreads, 0, st>>>(v, ops); break;
     }
 }
 
-template <typename ST, bool G, bool D>
+template <bool G, bool D>
 static void launch_edge4(int R, int grid, cudaStream_t st, const View &v, int pb, int cb, int mat, int tip,
                          int ws) {
     switch (R) {
-        case 1: k_edge4<ST, 1, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        case 2: k_edge4<ST, 2, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        case 3: k_edge4<ST, 3, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        case 4: k_edge4<ST, 4, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        case 5: k_edge4<ST, 5, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        case 6: k_edge4<ST, 6, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        case 7: k_edge4<ST, 7, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
-        default: k_edge4<ST, 8, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 1: k_edge4<1, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 2: k_edge4<2, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 3: k_edge4<3, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 4: k_edge4<4, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 5: k_edge4<5, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 6: k_edge4<6, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        case 7: k_edge4<7, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
+        default: k_edge4<8, G, D><<<grid, kThreads, 0, st>>>(v, pb, cb, mat, tip, ws); break;
     }
 }
 
@@ -190,14 +213,23 @@ static int ns_edge_tile(const Instance *I, size_t *smem) {
 
 static int set_smem_attrs() {
     const int big = 200 * 1024;
-    GB_CUDA(cudaFuncSetAttribute(k_cla_ns<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_cla_ns<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GB_CUDA(cudaFuncSetAttribute(k_cla_ns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GB_CUDA(cudaFuncSetAttribute(k_cla_ns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_pmats, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     return GB_SUCCESS;
+}
+
+// grid of a 4-state CLA level: tiles x ops, about 16 resident blocks per SM in total
+static dim3 cla4_grid(const Instance *I, int nops) {
+    const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
+    const int ppb = kThreads / G;
+    const int ntiles = (I->npat + ppb - 1) / ppb;
+    const int want = (16 * I->nsm + nops - 1) / nops;
+    return dim3(std::max(1, std::min(ntiles, want)), nops);
 }
 
 static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleEvery) {
@@ -214,17 +246,15 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             cudaEventRecord(e0, I->stream);
         }
         if (I->S == 4) {
-            const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
-            const int ppb = kThreads / G;
-            dim3 grid((I->npat + ppb - 1) / ppb, L.n);
-            if (I->mixed) launch_cla4<float, false>(I->R, grid, I->stream, v, L);
-            else launch_cla4<double, true>(I->R, grid, I->stream, v, L);
+            const dim3 grid = cla4_grid(I, L.n);
+            if (I->mixed) launch_cla4<false>(I->R, grid, I->stream, v, L);
+            else launch_cla4<true>(I->R, grid, I->stream, v, L);
         } else {
             size_t smem;
             const int tp = ns_cla_tile(I, &smem);
             dim3 grid((I->npat + tp - 1) / tp, L.n);
-            if (I->mixed) k_cla_ns<float, false><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
-            else k_cla_ns<double, true><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
+            if (I->mixed) k_cla_ns<false><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
+            else k_cla_ns<true><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
         }
         int rc = check_launch(I);
         if (rc) return rc;
@@ -232,6 +262,13 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             cudaEventRecord(e1, I->stream);
             I->ev.emplace_back(e0, e1);
             I->ev_updates.push_back((long long)L.n * I->npat);
+            // algorithmic bytes per pattern: internal-internal 3*R*S*b + 12,
+            // internal-tip 2*R*S*b + 9, tip-tip R*S*b + 6 (children read once, dest written once)
+            const double rsb = (double)I->R * I->S * I->elem;
+            double b = 0.0;
+            for (int i = 0; i < L.n; i++)
+                b += L.op[i].kind == kIntInt ? 3 * rsb + 12 : L.op[i].kind == kIntTip ? 2 * rsb + 9 : rsb + 6;
+            I->ev_bytes.push_back(b * I->npat);
         }
     }
     return GB_SUCCESS;
@@ -246,6 +283,7 @@ static void resolve_timing(Instance *I) {
         I->cla_ms += ms;
         I->cla_launches_timed++;
         I->cla_updates_timed += I->ev_updates[i];
+        I->cla_bytes_timed += I->ev_bytes[i];
         cudaEventDestroy(I->ev[i].first);
         cudaEventDestroy(I->ev[i].second);
     }
@@ -259,6 +297,7 @@ static void resolve_timing(Instance *I) {
     }
     I->ev.clear();
     I->ev_updates.clear();
+    I->ev_bytes.clear();
     I->ev_edge.clear();
 }
 
@@ -304,6 +343,25 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     I->elem = I->mixed ? 4 : 8;
     I->rank.assign(partialsBufferCount, 0);
     I->h_rates.assign(categoryCount, 1.0);
+    // FP64 segment: everything in the plain form; in the precision form room for
+    // max(128, npat/32) heavy patterns (rounded to the 128-pattern tile)
+    if (I->mixed) {
+        const int cap = std::max(128, (I->npat_pad / 32 + 127) / 128 * 128);
+        I->kpad_cap = std::min(cap, I->npat_pad);
+        I->kpad = 0;
+    } else {
+        I->kpad_cap = I->kpad = I->npat_pad;
+    }
+    {
+        const long long RS = (long long)I->R * I->S;
+        I->cla_bytes = (long long)I->kpad_cap * RS * 8 + (long long)(I->npat_pad - I->kpad_cap) * RS * 4;
+        I->cla_bytes = (I->cla_bytes + 255) / 256 * 256;
+    }
+    I->h_tips.assign((size_t)tipCount * patternCount, stateCount == 4 ? 15 : stateCount);
+    I->h_counts.assign(patternCount, 1);
+    I->h_cs.assign(patternCount, -1);
+    I->perm.resize(patternCount);
+    for (int q = 0; q < patternCount; q++) I->perm[q] = q;
     auto fail = [&](int rc) {
         if (I->stream) cudaStreamDestroy(I->stream);
         delete I;
@@ -315,8 +373,9 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     rc = set_smem_attrs();
     if (rc) return fail(rc);
     if (cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(GB_ERROR_GENERAL);
+    cudaDeviceGetAttribute(&I->nsm, cudaDevAttrMultiProcessorCount, resourceNumber);
     const size_t P = I->npat_pad;
-    const size_t cla_bytes = (size_t)I->nbuf * P * I->R * I->S * I->elem;
+    const size_t cla_bytes = (size_t)I->nbuf * I->cla_bytes;
     struct A {
         void **p;
         size_t n;
@@ -335,6 +394,8 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         {(void **)&I->d_block_sums, (size_t)kMaxScoreBlocks * 3 * sizeof(double)},
         {(void **)&I->d_result, 4 * sizeof(double)},
         {(void **)&I->d_site_lnl, P * sizeof(double)},
+        {(void **)&I->d_len, (size_t)I->nmat * sizeof(double)},
+        {(void **)&I->d_slots, (size_t)I->nmat * sizeof(NrSlot)},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, a.n) != cudaSuccess) {
@@ -359,6 +420,7 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     for (int i = 0; i < patternCount; i++) ones[i] = 1;
     cudaMemcpyAsync(I->d_counts, ones.data(), P * sizeof(int), cudaMemcpyHostToDevice, I->stream);
     cudaMemsetAsync(I->d_tips, stateCount == 4 ? 15 : stateCount, (size_t)I->ntip * P, I->stream);
+    cudaMemsetAsync(I->d_const, 0xff, P * sizeof(int), I->stream);
     std::vector<double> one(I->R, 1.0), pr(I->R, 1.0 / I->R), fr(I->S, 1.0 / I->S);
     cudaMemcpyAsync(I->d_rates, one.data(), I->R * sizeof(double), cudaMemcpyHostToDevice, I->stream);
     cudaMemcpyAsync(I->d_rprobs, pr.data(), I->R * sizeof(double), cudaMemcpyHostToDevice, I->stream);
@@ -391,9 +453,11 @@ int gb_finalize_instance(int instance) {
     cudaSetDevice(I->device);
     cudaStreamSynchronize(I->stream);
     resolve_timing(I);
+    if (I->graph_exec) cudaGraphExecDestroy(I->graph_exec);
+    if (I->graph) cudaGraphDestroy(I->graph);
     void *ptrs[] = {I->d_partials, I->d_scalers, I->d_tips, I->d_counts, I->d_const, I->d_mats,
                     I->d_eigen, I->d_freqs, I->d_rates, I->d_rprobs, I->d_status, I->d_block_sums,
-                    I->d_result, I->d_site_lnl};
+                    I->d_result, I->d_site_lnl, I->d_len, I->d_slots};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     cudaFreeHost(I->h_result);
@@ -407,48 +471,104 @@ int gb_finalize_instance(int instance) {
     return GB_SUCCESS;
 }
 
-int gb_set_tip_states(int instance, int tipIndex, const unsigned char *codes) {
-    Instance *I = get(instance);
-    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
-    if (tipIndex < 0 || tipIndex >= I->ntip || !codes) return GB_ERROR_OUT_OF_RANGE;
-    const int miss = I->S == 4 ? 15 : I->S;
-    for (int p = 0; p < I->npat; p++)
-        if (I->S == 4 ? (codes[p] & ~15) != 0 : codes[p] > miss) return GB_ERROR_OUT_OF_RANGE;
-    cudaSetDevice(I->device);
-    GB_CUDA(cudaMemcpyAsync(I->d_tips + (size_t)tipIndex * I->npat_pad, codes, I->npat, cudaMemcpyHostToDevice,
+}  // extern "C"
+
+namespace gb {
+
+static int upload_tip(Instance *I, int t) {
+    std::vector<uint8_t> row(I->npat);
+    const uint8_t *src = I->h_tips.data() + (size_t)t * I->npat;
+    for (int q = 0; q < I->npat; q++) row[q] = src[I->perm[q]];
+    GB_CUDA(cudaMemcpyAsync(I->d_tips + (size_t)t * I->npat_pad, row.data(), I->npat, cudaMemcpyHostToDevice,
                             I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
     return GB_SUCCESS;
 }
 
+static int upload_patterns(Instance *I) {
+    std::vector<int> c(I->npat), cs(I->npat);
+    for (int q = 0; q < I->npat; q++) {
+        c[q] = I->h_counts[I->perm[q]];
+        cs[q] = I->h_cs[I->perm[q]];
+    }
+    GB_CUDA(cudaMemcpyAsync(I->d_counts, c.data(), I->npat * sizeof(int), cudaMemcpyHostToDevice, I->stream));
+    GB_CUDA(cudaMemcpyAsync(I->d_const, cs.data(), I->npat * sizeof(int), cudaMemcpyHostToDevice, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    return GB_SUCCESS;
+}
+
+// precision form: patterns with count >= kHeavyCount go first (largest counts
+// first if they exceed the FP64 segment), everything else keeps its order
+static void make_permutation(Instance *I) {
+    std::vector<int> heavy, light;
+    for (int q = 0; q < I->npat; q++) (I->h_counts[q] >= kHeavyCount ? heavy : light).push_back(q);
+    if ((int)heavy.size() > I->kpad_cap) {
+        std::stable_sort(heavy.begin(), heavy.end(),
+                         [&](int a, int b) { return I->h_counts[a] > I->h_counts[b]; });
+        for (size_t i = I->kpad_cap; i < heavy.size(); i++) light.push_back(heavy[i]);
+        heavy.resize(I->kpad_cap);
+        std::sort(light.begin(), light.end());
+    }
+    I->kpad = heavy.empty() ? 0 : std::min(I->kpad_cap, ((int)heavy.size() + 127) / 128 * 128);
+    I->perm = heavy;
+    I->perm.insert(I->perm.end(), light.begin(), light.end());
+}
+
+}  // namespace gb
+
+extern "C" {
+
+int gb_set_tip_states(int instance, int tipIndex, const unsigned char *codes) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
+    if (tipIndex < 0 || tipIndex >= I->ntip || !codes) return GB_ERROR_OUT_OF_RANGE;
+    const int miss = I->S == 4 ? 15 : I->S;
+    for (int p = 0; p < I->npat; p++)
+        if (I->S == 4 ? (codes[p] & ~15) != 0 : codes[p] > miss) return GB_ERROR_OUT_OF_RANGE;
+    cudaSetDevice(I->device);
+    std::memcpy(I->h_tips.data() + (size_t)tipIndex * I->npat, codes, I->npat);
+    return upload_tip(I, tipIndex);
+}
+
 int gb_set_pattern_weights(int instance, const int *counts) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
+    for (int p = 0; p < I->npat; p++)
+        if (counts[p] < 0) return GB_ERROR_OUT_OF_RANGE;
     cudaSetDevice(I->device);
-    GB_CUDA(cudaMemcpyAsync(I->d_counts, counts, I->npat * sizeof(int), cudaMemcpyHostToDevice, I->stream));
-    GB_CUDA(cudaStreamSynchronize(I->stream));
-    return GB_SUCCESS;
+    I->h_counts.assign(counts, counts + I->npat);
+    if (I->mixed) {
+        const std::vector<int> old = I->perm;
+        make_permutation(I);
+        if (old != I->perm) {
+            for (int t = 0; t < I->ntip; t++) {
+                int rc = upload_tip(I, t);
+                if (rc) return rc;
+            }
+        }
+    }
+    return upload_patterns(I);
 }
 
 int gb_set_constant_patterns(int instance, int lastConst, const int *constStates) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
     if (lastConst >= I->npat || lastConst < -1) return GB_ERROR_OUT_OF_RANGE;
+    for (int p = 0; p <= lastConst; p++)
+        if (constStates[p] < 0 || constStates[p] > (I->S == 4 ? 15 : I->S - 1)) return GB_ERROR_OUT_OF_RANGE;
     cudaSetDevice(I->device);
     I->last_const = lastConst;
-    if (lastConst >= 0) {
-        for (int p = 0; p <= lastConst; p++)
-            if (constStates[p] < 0 || constStates[p] > (I->S == 4 ? 15 : I->S - 1)) return GB_ERROR_OUT_OF_RANGE;
-        GB_CUDA(cudaMemcpyAsync(I->d_const, constStates, (lastConst + 1) * sizeof(int), cudaMemcpyHostToDevice,
-                                I->stream));
-        GB_CUDA(cudaStreamSynchronize(I->stream));
-    }
-    return GB_SUCCESS;
+    for (int p = 0; p < I->npat; p++) I->h_cs[p] = p <= lastConst ? constStates[p] : -1;
+    return upload_patterns(I);
 }
 
 int gb_set_state_frequencies(int instance, const double *freqs) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
     cudaSetDevice(I->device);
     GB_CUDA(cudaMemcpyAsync(I->d_freqs, freqs, I->S * sizeof(double), cudaMemcpyHostToDevice, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
@@ -458,6 +578,7 @@ int gb_set_state_frequencies(int instance, const double *freqs) {
 int gb_set_category_rates(int instance, const double *rates) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
     cudaSetDevice(I->device);
     I->h_rates.assign(rates, rates + I->R);
     GB_CUDA(cudaMemcpyAsync(I->d_rates, rates, I->R * sizeof(double), cudaMemcpyHostToDevice, I->stream));
@@ -468,6 +589,7 @@ int gb_set_category_rates(int instance, const double *rates) {
 int gb_set_category_weights(int instance, const double *weights) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
     cudaSetDevice(I->device);
     GB_CUDA(cudaMemcpyAsync(I->d_rprobs, weights, I->R * sizeof(double), cudaMemcpyHostToDevice, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
@@ -477,6 +599,7 @@ int gb_set_category_weights(int instance, const double *weights) {
 int gb_set_invariant_sites(int instance, double pinv, int hasPinv) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
     if (!(pinv >= 0.0 && pinv < 1.0)) return GB_ERROR_OUT_OF_RANGE;
     I->pinv = pinv;
     I->has_pinv = hasPinv ? 1 : 0;
@@ -487,6 +610,7 @@ int gb_set_eigen_decomposition(int instance, int eigenIndex, const double *U, co
                                const double *lambda) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->version++;
     if (eigenIndex < 0 || eigenIndex >= I->neigen) return GB_ERROR_OUT_OF_RANGE;
     cudaSetDevice(I->device);
     const int S = I->S;
@@ -541,12 +665,17 @@ int gb_set_transition_matrix(int instance, int matrixIndex, const double *P, con
     return GB_SUCCESS;
 }
 
-int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int rescaleEvery) {
-    Instance *I = get(instance);
-    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
-    if (count < 0) return GB_ERROR_OUT_OF_RANGE;
-    if (count == 0) return GB_SUCCESS;
-    cudaSetDevice(I->device);
+}  // extern "C"
+
+namespace gb {
+
+// Normalise, validate and level a list of ClaOperations; applies GARLI's rank
+// rule (tree.cpp:7665-8598) to the instance's rank table as the ops would
+// execute and returns the per-level device op lists.
+static int prepare_ops(Instance *I, const gb_cla_operation *ops, int count, int rescaleEvery,
+                       std::vector<std::vector<DevOp>> &levels) {
+    levels.clear();
+    if (count <= 0) return GB_SUCCESS;
     std::vector<int> order(count);
     for (int i = 0; i < count; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(),
@@ -554,17 +683,14 @@ int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int
     const int nt = I->ntip, nb = I->nbuf;
     auto is_tip = [&](int b) { return b >= 0 && b < nt; };
     auto is_cla = [&](int b) { return b >= nt && b < nt + nb; };
-    std::vector<DevOp> level;
     int cur = ops[order[0]].opDepLevel;
-    for (int k = 0; k <= count; k++) {
-        if (k == count || ops[order[k]].opDepLevel != cur) {
-            int rc = launch_level(I, level, rescaleEvery);
-            if (rc) return rc;
-            level.clear();
-            if (k == count) break;
-            cur = ops[order[k]].opDepLevel;
-        }
+    levels.emplace_back();
+    for (int k = 0; k < count; k++) {
         const gb_cla_operation &o = ops[order[k]];
+        if (o.opDepLevel != cur) {
+            cur = o.opDepLevel;
+            levels.emplace_back();
+        }
         if (!is_cla(o.destClaIndex) || !(is_tip(o.childClaIndex1) || is_cla(o.childClaIndex1)) ||
             !(is_tip(o.childClaIndex2) || is_cla(o.childClaIndex2)) || o.transMatIndex1 < 0 ||
             o.transMatIndex1 >= I->nmat || o.transMatIndex2 < 0 || o.transMatIndex2 >= I->nmat)
@@ -594,7 +720,27 @@ int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int
         d.p2 = p2;
         d.rescale = (!I->mixed && rank >= rescaleEvery) ? 1 : 0;
         I->rank[dest] = d.rescale ? 0 : rank;
-        level.push_back(d);
+        levels.back().push_back(d);
+    }
+    return GB_SUCCESS;
+}
+
+}  // namespace gb
+
+extern "C" {
+
+int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int rescaleEvery) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (count < 0) return GB_ERROR_OUT_OF_RANGE;
+    if (count == 0) return GB_SUCCESS;
+    cudaSetDevice(I->device);
+    std::vector<std::vector<DevOp>> levels;
+    int rc = prepare_ops(I, ops, count, rescaleEvery, levels);
+    if (rc) return rc;
+    for (auto &lv : levels) {
+        rc = launch_level(I, lv, rescaleEvery);
+        if (rc) return rc;
     }
     return GB_SUCCESS;
 }
@@ -620,22 +766,22 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
     if (I->S == 4) {
         nblocks = std::min(kMaxScoreBlocks, (I->npat + kThreads - 1) / kThreads);
         if (I->mixed) {
-            if (D) launch_edge4<float, false, true>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
-            else launch_edge4<float, false, false>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
+            if (D) launch_edge4<false, true>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
+            else launch_edge4<false, false>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
         } else {
-            if (D) launch_edge4<double, true, true>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
-            else launch_edge4<double, true, false>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
+            if (D) launch_edge4<true, true>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
+            else launch_edge4<true, false>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
         }
     } else {
         size_t smem;
         const int tp = ns_edge_tile(I, &smem);
         nblocks = std::min(kMaxScoreBlocks, (I->npat + tp - 1) / tp);
         if (I->mixed) {
-            if (D) k_edge_ns<float, false, true><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
-            else k_edge_ns<float, false, false><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
+            if (D) k_edge_ns<false, true><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
+            else k_edge_ns<false, false><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
         } else {
-            if (D) k_edge_ns<double, true, true><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
-            else k_edge_ns<double, true, false><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
+            if (D) k_edge_ns<true, true><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
+            else k_edge_ns<true, false><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
         }
     }
     int rc = check_launch(I);
@@ -677,8 +823,10 @@ int gb_get_site_log_likelihoods(int instance, double *out) {
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
     if (!I->site_valid) return GB_ERROR_GENERAL;
     cudaSetDevice(I->device);
-    GB_CUDA(cudaMemcpyAsync(out, I->d_site_lnl, I->npat * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    std::vector<double> tmp(I->npat);
+    GB_CUDA(cudaMemcpyAsync(tmp.data(), I->d_site_lnl, I->npat * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
+    for (int q = 0; q < I->npat; q++) out[I->perm[q]] = tmp[q];
     return GB_SUCCESS;
 }
 
@@ -688,16 +836,17 @@ int gb_get_partials(int instance, int bufferIndex, double *out) {
     const int b = bufferIndex - I->ntip;
     if (b < 0 || b >= I->nbuf) return GB_ERROR_OUT_OF_RANGE;
     cudaSetDevice(I->device);
-    const size_t n = (size_t)I->npat * I->R * I->S;
-    const char *src = (const char *)I->d_partials + (size_t)b * I->cla_stride() * I->elem;
-    if (!I->mixed) {
-        GB_CUDA(cudaMemcpyAsync(out, src, n * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
-        GB_CUDA(cudaStreamSynchronize(I->stream));
-    } else {
-        std::vector<float> tmp(n);
-        GB_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost, I->stream));
-        GB_CUDA(cudaStreamSynchronize(I->stream));
-        for (size_t i = 0; i < n; i++) out[i] = tmp[i];
+    const int RS = I->R * I->S;
+    std::vector<char> raw(I->cla_bytes);
+    GB_CUDA(cudaMemcpyAsync(raw.data(), (const char *)I->d_partials + (size_t)b * I->cla_bytes, I->cla_bytes,
+                            cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    const double *d64 = reinterpret_cast<const double *>(raw.data());
+    const float *d32 = reinterpret_cast<const float *>(raw.data() + (size_t)I->kpad * RS * 8);
+    for (int q = 0; q < I->npat; q++) {
+        double *dst = out + (size_t)I->perm[q] * RS;
+        for (int k = 0; k < RS; k++)
+            dst[k] = q < I->kpad ? d64[(size_t)q * RS + k] : (double)d32[(size_t)(q - I->kpad) * RS + k];
     }
     return GB_SUCCESS;
 }
@@ -708,9 +857,11 @@ int gb_get_scale_factors(int instance, int bufferIndex, int *out) {
     const int b = bufferIndex - I->ntip;
     if (b < 0 || b >= I->nbuf) return GB_ERROR_OUT_OF_RANGE;
     cudaSetDevice(I->device);
-    GB_CUDA(cudaMemcpyAsync(out, I->d_scalers + (size_t)b * I->npat_pad, I->npat * sizeof(int),
+    std::vector<int> tmp(I->npat);
+    GB_CUDA(cudaMemcpyAsync(tmp.data(), I->d_scalers + (size_t)b * I->npat_pad, I->npat * sizeof(int),
                             cudaMemcpyDeviceToHost, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
+    for (int q = 0; q < I->npat; q++) out[I->perm[q]] = tmp[q];
     return GB_SUCCESS;
 }
 
@@ -738,7 +889,7 @@ int gb_get_partials_pool(int instance, void **devicePtr, long long *bytes) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
     if (devicePtr) *devicePtr = I->d_partials;
-    if (bytes) *bytes = (long long)I->nbuf * I->cla_stride() * I->elem;
+    if (bytes) *bytes = (long long)I->nbuf * I->cla_bytes;
     return GB_SUCCESS;
 }
 
@@ -781,12 +932,13 @@ int gb_set_kernel_timing(int instance, int on) {
     cudaSetDevice(I->device);
     resolve_timing(I);
     I->timing = on != 0;
-    I->cla_ms = I->edge_ms = 0.0;
+    I->cla_ms = I->edge_ms = I->cla_bytes_timed = 0.0;
     I->cla_launches_timed = I->cla_updates_timed = I->edge_timed = 0;
     return GB_SUCCESS;
 }
 
-// out: [0] CLA-kernel ms, [1] CLA launches, [2] pattern-updates, [3] edge ms, [4] edge evals
+// out: [0] CLA-kernel ms, [1] CLA launches, [2] pattern-updates, [3] edge ms, [4] edge evals,
+//      [5] algorithmic bytes of the timed CLA launches
 int gb_get_kernel_timing(int instance, double *out) {
     Instance *I = get(instance);
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
@@ -797,6 +949,291 @@ int gb_get_kernel_timing(int instance, double *out) {
     out[2] = (double)I->cla_updates_timed;
     out[3] = I->edge_ms;
     out[4] = (double)I->edge_timed;
+    out[5] = I->cla_bytes_timed;
+    return GB_SUCCESS;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Graph-resident branch-optimisation pass (OptimizeAllBranches on the device)
+// ===========================================================================
+namespace gb {
+
+static unsigned long long fnv(unsigned long long h, const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+static void *cla4_func(int R, bool garli) {
+#define GB_CASE(r) \
+    case r: return garli ? (void *)k_cla4<r, true> : (void *)k_cla4<r, false>;
+    switch (R) {
+        GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
+    }
+#undef GB_CASE
+}
+static void *edge4_deriv_func(int R, bool garli) {
+#define GB_CASE(r) \
+    case r: return garli ? (void *)k_edge4<r, true, true> : (void *)k_edge4<r, false, true>;
+    switch (R) {
+        GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
+    }
+#undef GB_CASE
+}
+
+struct GraphBuilder {
+    cudaGraph_t g;
+    int nodes = 0;
+    int add(cudaGraph_t graph, cudaGraphNode_t *prev, void *func, dim3 grid, size_t smem, void **args) {
+        cudaKernelNodeParams kp = {};
+        kp.func = func;
+        kp.gridDim = grid;
+        kp.blockDim = dim3(kThreads);
+        kp.sharedMemBytes = (unsigned)smem;
+        kp.kernelParams = args;
+        cudaGraphNode_t n;
+        cudaError_t e = cudaGraphAddKernelNode(&n, graph, *prev ? prev : nullptr, *prev ? 1 : 0, &kp);
+        if (e != cudaSuccess) {
+            g_last_error = std::string("cudaGraphAddKernelNode: ") + cudaGetErrorString(e);
+            return GB_ERROR_GENERAL;
+        }
+        *prev = n;
+        nodes++;
+        return GB_SUCCESS;
+    }
+};
+
+static void *nr_iter4_func(int R, bool garli) {
+#define GB_CASE(r) \
+    case r: return garli ? (void *)k_nr_iter4<r, true> : (void *)k_nr_iter4<r, false>;
+    switch (R) {
+        GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
+    }
+#undef GB_CASE
+}
+
+// levels[b] = the prepared (levelled, rank-flagged) CLA updates of branch b
+static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
+                            const std::vector<std::vector<std::vector<DevOp>>> &levels, int rescaleEvery,
+                            NrParams prm) {
+    if (I->graph_exec) cudaGraphExecDestroy(I->graph_exec);
+    if (I->graph) cudaGraphDestroy(I->graph);
+    I->graph_exec = nullptr;
+    I->graph = nullptr;
+    GraphBuilder B;
+    GB_CUDA(cudaGraphCreate(&B.g, 0));
+    I->graph = B.g;
+    View v = make_view(I);
+    v.rescale_every = rescaleEvery;
+    cudaGraphNode_t prev = nullptr;
+    const bool dna = I->S == 4;
+    const bool garli = !I->mixed;
+    size_t ns_smem = 0, ns_edge_smem = 0;
+    int ns_tp = 0, ns_edge_tp = 0;
+    if (!dna) {
+        ns_tp = ns_cla_tile(I, &ns_smem);
+        ns_edge_tp = ns_edge_tile(I, &ns_edge_smem);
+    }
+    const int nblocks = dna ? std::min(kMaxScoreBlocks, (I->npat + kThreads - 1) / kThreads)
+                            : std::min(kMaxScoreBlocks, (I->npat + ns_edge_tp - 1) / ns_edge_tp);
+    const size_t pmat_smem = 3 * (size_t)I->R * I->S * sizeof(double);
+    int rc;
+    {
+        int n = I->nmat;
+        void *args[] = {&I->d_slots, &n};
+        rc = B.add(B.g, &prev, (void *)k_nr_reset, dim3((n + kThreads - 1) / kThreads), 0, args);
+        if (rc) return rc;
+    }
+    for (int b = 0; b < nbr; b++) {
+        const gb_nr_branch &nb = br[b];
+        for (auto &lv : levels[b]) {
+            for (size_t c = 0; c < lv.size(); c += kMaxLevelOps) {
+                LevelOps L;
+                L.n = (int)std::min<size_t>(kMaxLevelOps, lv.size() - c);
+                for (int i = 0; i < L.n; i++) L.op[i] = lv[c + i];
+                if (dna) {
+                    void *args[] = {&v, &L};
+                    rc = B.add(B.g, &prev, cla4_func(I->R, garli), cla4_grid(I, L.n), 0, args);
+                } else {
+                    int S = I->S, R = I->R, tp = ns_tp;
+                    void *args[] = {&v, &L, &S, &R, &tp};
+                    rc = B.add(B.g, &prev, garli ? (void *)k_cla_ns<true> : (void *)k_cla_ns<false>,
+                               dim3((I->npat + ns_tp - 1) / ns_tp, L.n), ns_smem, args);
+                }
+                if (rc) return rc;
+            }
+        }
+        // Newton loop of this branch: WHILE(not converged) { one iteration }
+        NrSlot *slot = I->d_slots + nb.transMatIndex;
+        int mat = nb.transMatIndex;
+        cudaGraphConditionalHandle h;
+        GB_CUDA(cudaGraphConditionalHandleCreate(&h, B.g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        GB_CUDA(cudaGraphAddNode(&cn, B.g, prev ? &prev : nullptr, prev ? 1 : 0, &cp));
+        prev = cn;
+        B.nodes++;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        cudaGraphNode_t bprev = nullptr;
+        int pb = nb.partialIndex - I->ntip;
+        int tip = nb.childIndex < I->ntip;
+        int cb = tip ? nb.childIndex : nb.childIndex - I->ntip;
+        if (dna) {
+            long long es = I->eig_stride();
+            void *args[] = {&v, &slot, &pb, &cb, &mat, &tip, &prm, &I->d_len, &I->d_eigen, &es, &I->d_rates, &h};
+            rc = B.add(body, &bprev, nr_iter4_func(I->R, garli), dim3(nblocks), pmat_smem, args);
+            if (rc) return rc;
+        } else {
+            int ws = 0;
+            {
+                int S = I->S, R = I->R, tp = ns_edge_tp;
+                void *args[] = {&v, &pb, &cb, &mat, &tip, &ws, &S, &R, &tp};
+                rc = B.add(body, &bprev, garli ? (void *)k_edge_ns<true, true> : (void *)k_edge_ns<false, true>,
+                           dim3(nblocks), ns_edge_smem, args);
+                if (rc) return rc;
+            }
+            {
+                int nbk = nblocks;
+                void *args[] = {&slot, &I->d_block_sums, &nbk, &I->d_len, &mat, &prm, &h};
+                rc = B.add(body, &bprev, (void *)k_nr_decide, dim3(1), 0, args);
+                if (rc) return rc;
+            }
+            {
+                long long es = I->eig_stride(), ms = I->mat_stride();
+                int S = I->S, R = I->R, hp = I->has_pinv, e0 = 0;
+                double pinv = I->pinv;
+                void *args[] = {&I->d_eigen, &es, &S, &R, &I->d_rates, &pinv, &hp, &mat, &e0, &I->d_len, &I->d_mats, &ms};
+                rc = B.add(body, &bprev, (void *)k_pmat_len, dim3(1), pmat_smem, args);
+                if (rc) return rc;
+            }
+        }
+    }
+    cudaError_t e = cudaGraphInstantiate(&I->graph_exec, B.g, 0);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+        return GB_ERROR_GENERAL;
+    }
+    I->graph_nodes = B.nodes;
+    return GB_SUCCESS;
+}
+
+}  // namespace gb
+
+extern "C" {
+
+int gb_set_branch_lengths(int instance, const double *lengths, int count) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (count < 0 || count > I->nmat) return GB_ERROR_OUT_OF_RANGE;
+    cudaSetDevice(I->device);
+    GB_CUDA(cudaMemcpyAsync(I->d_len, lengths, count * sizeof(double), cudaMemcpyHostToDevice, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    return GB_SUCCESS;
+}
+
+int gb_get_branch_lengths(int instance, double *lengths, int count) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (count < 0 || count > I->nmat) return GB_ERROR_OUT_OF_RANGE;
+    cudaSetDevice(I->device);
+    GB_CUDA(cudaMemcpyAsync(lengths, I->d_len, count * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    return GB_SUCCESS;
+}
+
+int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, const gb_cla_operation *ops,
+                   int opCount, int rescaleEvery, double precision, double minLength, double maxLength,
+                   double *out) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (branchCount < 0 || opCount < 0 || !(precision > 0.0) || !(minLength > 0.0) || !(maxLength > minLength))
+        return GB_ERROR_OUT_OF_RANGE;
+    for (int b = 0; b < branchCount; b++) {
+        const gb_nr_branch &nb = branches[b];
+        if (nb.transMatIndex < 0 || nb.transMatIndex >= I->nmat || nb.firstOp < 0 || nb.opCount < 0 ||
+            nb.firstOp + nb.opCount > opCount || nb.partialIndex < I->ntip ||
+            nb.partialIndex >= I->ntip + I->nbuf || nb.childIndex < 0 || nb.childIndex >= I->ntip + I->nbuf)
+            return GB_ERROR_OUT_OF_RANGE;
+    }
+    cudaSetDevice(I->device);
+    NrParams prm{precision, minLength, maxLength};
+    // prepare every branch's CLA updates (this applies the rank rule, as executing them would)
+    const std::vector<int> rank_before = I->rank;
+    std::vector<std::vector<std::vector<DevOp>>> levels(branchCount);
+    unsigned long long key = 1469598103934665603ULL;
+    for (int b = 0; b < branchCount; b++) {
+        int rc = prepare_ops(I, ops + branches[b].firstOp, branches[b].opCount, rescaleEvery, levels[b]);
+        if (rc) {
+            I->rank = rank_before;
+            return rc;
+        }
+        for (auto &lv : levels[b]) key = fnv(key, lv.data(), sizeof(DevOp) * lv.size());
+        key = fnv(key, &branches[b], sizeof(gb_nr_branch));
+    }
+    key = fnv(key, &rescaleEvery, sizeof(int));
+    key = fnv(key, &prm, sizeof(prm));
+    key = fnv(key, &I->version, sizeof(I->version));
+    if (key != I->graph_key || !I->graph_exec) {
+        int rc = build_pass_graph(I, branches, branchCount, levels, rescaleEvery, prm);
+        if (rc) {
+            I->rank = rank_before;
+            I->graph_key = 0;
+            return rc;
+        }
+        I->graph_key = key;
+    }
+    GB_CUDA(cudaGraphLaunch(I->graph_exec, I->stream));
+    I->launches += I->graph_nodes;
+    std::vector<NrSlot> slots(I->nmat);
+    GB_CUDA(cudaMemcpyAsync(slots.data(), I->d_slots, I->nmat * sizeof(NrSlot), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    double improve = 0.0, last = 0.0;
+    long long evals = 0;
+    for (int b = 0; b < branchCount; b++) {
+        const NrSlot &sl = slots[branches[b].transMatIndex];
+        improve += sl.st.totalEstImprove;
+        evals += sl.evals;
+        last = sl.lnL;
+    }
+    if (out) {
+        out[0] = improve;
+        out[1] = last;
+        out[2] = (double)evals;
+    }
+    I->site_valid = true;
+    if (*I->h_status & kStatusRescaleRetry) {
+        GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        I->graph_key = 0;
+        return GB_ERROR_RESCALE_RETRY;
+    }
+    return GB_SUCCESS;
+}
+
+int gb_get_newton_state(int instance, int matrixIndex, double *out) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (matrixIndex < 0 || matrixIndex >= I->nmat) return GB_ERROR_OUT_OF_RANGE;
+    cudaSetDevice(I->device);
+    NrSlot sl;
+    GB_CUDA(cudaMemcpyAsync(&sl, I->d_slots + matrixIndex, sizeof(NrSlot), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    out[0] = sl.st.v;
+    out[1] = sl.st.totalEstImprove;
+    out[2] = sl.lnL;
+    out[3] = sl.d1;
+    out[4] = sl.d2;
+    out[5] = sl.evals;
     return GB_SUCCESS;
 }
 

@@ -15,9 +15,20 @@ namespace gb {
 template <typename ST>
 __device__ __forceinline__ double ldv(const ST *p) { return (double)__ldg(p); }
 
+// copy n consecutive CLA values of buffer b starting at pattern p0 into shared memory
+__device__ __forceinline__ void tile_load(const View &v, int b, int p0, int RS, int n, double *dst) {
+    if (p0 < v.kpad) {
+        const double *src = cla_ptr<double>(v, b, p0, RS);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = ldv<double>(src + i);
+    } else {
+        const float *src = cla_ptr<float>(v, b, p0, RS);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = ldv<float>(src + i);
+    }
+}
+
 // dynamic shared memory layout for k_cla_ns:
 //   PL[R*S*S], PR[R*S*S], A[TP*R*S], B[TP*R*S], D[TP*R*S], mx[TP], mlt[TP]
-template <typename ST, bool GARLI_SCALE>
+template <bool GARLI_SCALE>
 __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S, int R, int TP) {
     extern __shared__ double sm[];
     const DevOp op = ops.op[blockIdx.y];
@@ -32,15 +43,8 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S
     }
     const int p0 = blockIdx.x * TP;
     const int np = min(TP, v.npat - p0);
-    const ST *base = reinterpret_cast<const ST *>(v.partials);
-    if (op.kind != kTipTip) {
-        const ST *ca = base + (long long)op.c1 * v.cla_stride + (long long)p0 * RS;
-        for (int i = threadIdx.x; i < np * RS; i += blockDim.x) A[i] = ldv<ST>(ca + i);
-    }
-    if (op.kind == kIntInt) {
-        const ST *cb = base + (long long)op.c2 * v.cla_stride + (long long)p0 * RS;
-        for (int i = threadIdx.x; i < np * RS; i += blockDim.x) B[i] = ldv<ST>(cb + i);
-    }
+    if (op.kind != kTipTip) tile_load(v, op.c1, p0, RS, np * RS, A);
+    if (op.kind == kIntInt) tile_load(v, op.c2, p0, RS, np * RS, B);
     __syncthreads();
     for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
         const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
@@ -99,19 +103,25 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S
         v.scalers[(long long)op.dest * v.npat_pad + p] = m;
     }
     __syncthreads();
-    ST *dst = reinterpret_cast<ST *>(v.partials) + (long long)op.dest * v.cla_stride + (long long)p0 * RS;
-    for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
-        const double mult = mx[o / RS];
-        double val = D[o];
-        if (mult != 1.0) val = mul(val, mult);
-        dst[o] = (ST)val;
+    if (p0 < v.kpad) {
+        double *dst = cla_ptr<double>(v, op.dest, p0, RS);
+        for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
+            const double mult = mx[o / RS];
+            dst[o] = mult != 1.0 ? mul(D[o], mult) : D[o];
+        }
+    } else {
+        float *dst = cla_ptr<float>(v, op.dest, p0, RS);
+        for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
+            const double mult = mx[o / RS];
+            dst[o] = (float)(mult != 1.0 ? mul(D[o], mult) : D[o]);
+        }
     }
 }
 
 // Edge evaluation for S states: per-(pattern, rate, from) terms computed in
 // parallel, then summed per pattern in the reference's order.
 // dynamic smem: M[3*R*S*S], C[TP*R*S], Pp[TP*R*S], T[3*TP*R*S], freqs[S], rp[R]
-template <typename ST, bool GARLI_SCALE, bool DERIV>
+template <bool GARLI_SCALE, bool DERIV>
 __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf, int mat, int child_tip,
                                                       int write_sites, int S, int R, int TP) {
     extern __shared__ double sm[];
@@ -121,19 +131,12 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
     for (int i = threadIdx.x; i < (DERIV ? 3 : 1) * RSS; i += blockDim.x) M[i] = mp[i];
     for (int i = threadIdx.x; i < S; i += blockDim.x) F[i] = v.freqs[i];
     for (int i = threadIdx.x; i < R; i += blockDim.x) RP[i] = v.rate_probs[i];
-    const ST *base = reinterpret_cast<const ST *>(v.partials);
     double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
     for (int p0 = blockIdx.x * TP; p0 < v.npat; p0 += gridDim.x * TP) {
         const int np = min(TP, v.npat - p0);
         __syncthreads();
-        {
-            const ST *pa = base + (long long)pbuf * v.cla_stride + (long long)p0 * RS;
-            for (int i = threadIdx.x; i < np * RS; i += blockDim.x) Pp[i] = ldv<ST>(pa + i);
-            if (!child_tip) {
-                const ST *ca = base + (long long)cbuf * v.cla_stride + (long long)p0 * RS;
-                for (int i = threadIdx.x; i < np * RS; i += blockDim.x) C[i] = ldv<ST>(ca + i);
-            }
-        }
+        tile_load(v, pbuf, p0, RS, np * RS, Pp);
+        if (!child_tip) tile_load(v, cbuf, p0, RS, np * RS, C);
         __syncthreads();
         for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
             const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
             }
             const int m1 = v.scalers[(long long)pbuf * v.npat_pad + p];
             const int m2 = child_tip ? 0 : v.scalers[(long long)cbuf * v.npat_pad + p];
-            if (v.has_pinv && p <= v.last_const) {
+            if (v.has_pinv && v.const_states[p] >= 0) {
                 const double pf = mul(v.pinv, F[v.const_states[p]]);
                 if (GARLI_SCALE) {
                     if (DERIV) {

@@ -24,10 +24,9 @@ struct TransOps {
 // P_ij = max(0, sum_k (U_ik Uinv_kj) e_k) with the k sum sequential.
 // eig layout per eigen index: [lambda (S) | U (S*S) | Uinv (S*S)], lambda pre-scaled
 // by the blen multiplier.
-__global__ void __launch_bounds__(kThreads) k_pmats(const double *eig, long long eig_stride, int S, int R,
-                                                    const double *rates, double pinv, int has_pinv,
-                                                    TransOps ops, double *mats, long long mat_stride) {
-    const TransOp op = ops.op[blockIdx.x];
+__device__ __forceinline__ void pmat_body(const double *eig, long long eig_stride, int S, int R,
+                                          const double *rates, double pinv, int has_pinv, const TransOp op,
+                                          double *mats, long long mat_stride) {
     extern __shared__ double sh[];
     double *ex = sh, *d1e = ex + R * S, *d2e = d1e + R * S;
     const double *lam = eig + (long long)op.eigen * eig_stride;
@@ -62,6 +61,26 @@ __global__ void __launch_bounds__(kThreads) k_pmats(const double *eig, long long
             out[2 * R * SS + idx] = s2;
         }
     }
+}
+
+__global__ void __launch_bounds__(kThreads) k_pmats(const double *eig, long long eig_stride, int S, int R,
+                                                    const double *rates, double pinv, int has_pinv,
+                                                    TransOps ops, double *mats, long long mat_stride) {
+    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, ops.op[blockIdx.x], mats, mat_stride);
+}
+
+// P(t), dP/dt, d2P/dt2 of one matrix whose branch length lives on the device
+// (the Newton iterations of a device-side optimisation pass)
+__global__ void __launch_bounds__(kThreads) k_pmat_len(const double *eig, long long eig_stride, int S, int R,
+                                                       const double *rates, double pinv, int has_pinv, int dest,
+                                                       int eigen, const double *lengths, double *mats,
+                                                       long long mat_stride) {
+    TransOp op;
+    op.dest = dest;
+    op.eigen = eigen;
+    op.derivs = 1;
+    op.t = lengths[dest];
+    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, op, mats, mat_stride);
 }
 
 // Sum the per-block partial sums of an edge evaluation (nblocks x 3) into

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/garli_b200.h"
+#include "gb_newton.h"
 
 namespace {
 
@@ -40,6 +41,7 @@ struct Tree {
     double minBrlen = 1e-8, maxBrlen = 100.0;  // defs.h:106-107
     long long nOps = 0, nPatUpdates = 0, nEdge = 0, nScores = 0, nRetries = 0;
     int npat = 0;
+    bool deviceNewton = true;  // OptimizeAllBranches as one device graph (gb_newton_pass)
 
     bool internal(int nd) const { return nd == 0 || nd > ntax; }
     int hidx(int nd, int which) const { return nd * 3 + which; }
@@ -290,145 +292,21 @@ int score(Tree &t, int root, double *lnl) {
     return rc;
 }
 
-// NewtonRaphsonOptimizeBranchLength, optimization.cpp:1359-1971 (FP64 build,
-// default exit rule)
+// NewtonRaphsonOptimizeBranchLength, optimization.cpp:1359-1971: derivative
+// evaluations on the engine, one gb::nr_step per iteration (gb_newton.h).
 int nr_optimize(Tree &t, double precision1, int nd, double *result) {
-    const double min_brlen = t.minBrlen, max_brlen = t.maxBrlen;
-    double totalEstImprove = 0.0;
-    int iter = 0;
-    const double v_onEntry = t.dlen[nd];
-    double v = t.dlen[nd], v_prev = t.dlen[nd];
-    int negProposalNum = 0;
-    double knownMin = min_brlen, knownMax = max_brlen;
-    double initialL = 0.0;
+    gb::NrState st;
+    gb::nr_init(st, t.dlen[nd], t.minBrlen, t.maxBrlen);
     double out[3];
-    auto done = [&](double r) {
-        *result = r;
-        return GB_SUCCESS;
-    };
     for (;;) {
         int rc = run_request(t, false, nd, out);
         if (rc) return rc;
-        if (iter == 0) initialL = t.lnL;
-        const double d1 = out[1], d2 = out[2], dlen = t.dlen[nd];
-        const double estDeltaNR = -d1 / d2;
-        const double estScoreDelta = d1 * estDeltaNR + (d2 * estDeltaNR * estDeltaNR * 0.5);
-        if (d1 <= 0.0 && dlen < knownMax) knownMax = dlen;
-        else if (d1 > 0.0 && dlen > knownMin) knownMin = dlen;
-        if (d2 >= 0.0) {
-            double proposed;
-            if (d1 <= 0.0) {
-                if (fp_equals(dlen, min_brlen, 1.0e-8)) {
-                    if (t.lnL < initialL - std::pow(10.0, -6.0 + std::ceil(std::log10(-t.lnL)))) {
-                        set_blen(t, nd, v_onEntry);
-                        totalEstImprove = 0.0;
-                        rc = score(t, 0, nullptr);
-                        if (rc) return rc;
-                    }
-                    return done(totalEstImprove);
-                }
-                if (knownMin == min_brlen) {
-                    if (dlen <= 1.0e-4) proposed = min_brlen;
-                    else if (dlen <= 0.005) proposed = 1.0e-4;
-                    else if (dlen <= 0.05) proposed = dlen * 0.1;
-                    else proposed = dlen * 0.25;
-                } else
-                    proposed = (knownMin + dlen) * 0.5;
-                if (iter > 0 || proposed == min_brlen) {
-                    const double estImp = d1 * (proposed - dlen) + (d2 * (proposed - dlen) * (proposed - dlen) * 0.5);
-                    if (estImp < precision1 && t.lnL >= initialL - 1.0e-4) return done(totalEstImprove);
-                }
-            } else {
-                if (knownMax == max_brlen) {
-                    if (dlen < 0.1) proposed = dlen * 10.0;
-                    else proposed = std::fmin(dlen * 2.0, max_brlen);
-                } else
-                    proposed = (knownMax + dlen) * 0.5;
-                if (iter > 0) {
-                    const double estImp = d1 * (proposed - dlen) + (d2 * (proposed - dlen) * (proposed - dlen) * 0.5);
-                    if (estImp < precision1 && t.lnL >= initialL - 1.0e-4) return done(totalEstImprove);
-                }
-            }
-            v = proposed;
-            totalEstImprove += precision1;
-        } else {
-            if (d1 < 0.0 && fp_equals(dlen, min_brlen, 1.0e-8)) return done(totalEstImprove);
-            if (d1 > 0.0 && fp_equals(dlen, max_brlen, 1.0e-8)) return done(totalEstImprove);
-            const double tol = (iter < 10 ? 1 : iter) * std::fmax(1.0e-7, DBL_EPSILON * 10.0);
-            if (estScoreDelta < precision1 && (iter == 0 || t.lnL + tol >= initialL)) return done(totalEstImprove);
-            bool noNR = false;
-            if (iter > 10) {
-                if (d1 > 0.0) {
-                    if (fp_equals(knownMax, max_brlen, 1e-8)) {
-                        if ((iter > 20) && (dlen > (max_brlen / 2.0))) v = max_brlen;
-                        else if (v < 0.2) v = std::fmin((v + max_brlen) * 0.5, v * 5.0);
-                        else v = std::fmin((v + max_brlen) * 0.5, v * 2.0);
-                        noNR = true;
-                    } else if (((iter - 20) > 0) && ((iter - 20) % 10 == 0)) {
-                        v = std::fmin((v + knownMax) * 0.5, v * 100.0);
-                    }
-                } else if (fp_equals(knownMin, min_brlen, 1e-8)) {
-                    v = (iter > 20) ? min_brlen : (v + min_brlen) * 0.5;
-                    noNR = true;
-                }
-            }
-            if (!noNR) v += estDeltaNR;
-            if (v <= knownMin) {
-                negProposalNum++;
-                if (knownMin == min_brlen) {
-                    const double dm = min_brlen - dlen;
-                    const double sdm = (dm * d1 + (dm * dm * d2 * 0.5));
-                    if (sdm < precision1) return done(totalEstImprove);
-                    if (negProposalNum == 1 && dlen > 1e-4 && v_prev != 1e-4) {
-                        if (dlen < .005) v = 1e-4;
-                        else if (dlen < 0.05) v = dlen * 0.1;
-                        else v = dlen * 0.25;
-                        const double delta = v - dlen;
-                        totalEstImprove += (delta * d1 + (delta * delta * d2 * 0.5));
-                    } else {
-                        v = min_brlen;
-                        totalEstImprove += sdm;
-                    }
-                } else {
-                    const double proposed = (knownMin + dlen) * 0.5;
-                    const double dm = proposed - dlen;
-                    const double sdm = (dm * d1 + (dm * dm * d2 * 0.5));
-                    if (sdm < precision1) return done(totalEstImprove);
-                    v = proposed;
-                    totalEstImprove += sdm;
-                }
-            } else if (v >= knownMax) {
-                if (knownMax == max_brlen) {
-                    const double dm = max_brlen - dlen;
-                    const double sdm = (dm * d1 + (dm * dm * d2 * 0.5));
-                    if (sdm < precision1) return done(totalEstImprove);
-                    v = max_brlen;
-                    totalEstImprove += sdm;
-                } else {
-                    const double proposed = (knownMax + dlen) * 0.5;
-                    const double dm = proposed - dlen;
-                    const double sdm = (dm * d1 + (dm * dm * d2 * 0.5));
-                    if (sdm < precision1) return done(totalEstImprove);
-                    v = proposed;
-                    totalEstImprove += sdm;
-                }
-            } else
-                totalEstImprove += estScoreDelta;
-        }
-        set_blen(t, nd, v);
-        v_prev = v;
-        iter++;
-        if (iter > 100) {
-            double l;
-            rc = score(t, t.anc[nd], &l);
-            if (rc) return rc;
-            if (t.lnL > initialL) return done(totalEstImprove);
-            set_blen(t, nd, v_onEntry);
-            rc = score(t, 0, nullptr);
-            if (rc) return rc;
-            return done(0.0);
-        }
+        const int fin = gb::nr_step(st, out[1], out[2], out[0], precision1, t.minBrlen, t.maxBrlen);
+        if (st.v != t.dlen[nd]) set_blen(t, nd, st.v);
+        if (fin) break;
     }
+    *result = st.totalEstImprove;
+    return GB_SUCCESS;
 }
 
 // RecursivelyOptimizeBranches, optimization.cpp:1042-1062
@@ -449,6 +327,92 @@ int rec_opt(Tree &t, int nd, double prec, int radius, bool dontGoNext, bool igno
         if (rc) return rc;
     }
     return GB_SUCCESS;
+}
+
+// Traversal order of OptimizeAllBranches -> RecursivelyOptimizeBranches with
+// ignoreDelta = true and an unbounded radius (optimization.cpp:97-105, :1042-1062)
+void pass_order(const Tree &t, int nd, bool dontGoNext, std::vector<int> &order, std::vector<char> &seen) {
+    if (!seen[nd]) {
+        seen[nd] = 1;
+        order.push_back(nd);
+    }
+    if (t.left[nd] >= 0) pass_order(t, t.left[nd], false, order, seen);
+    if (t.next[nd] >= 0 && !dontGoNext && !seen[t.next[nd]]) pass_order(t, t.next[nd], false, order, seen);
+}
+
+// OptimizeAllBranches as one device graph.  The plan assumes every branch
+// moves: its sweep (SweepDirtynessOverTree) is applied after each branch, so
+// a CLA that GARLI would have reused is recomputed from identical inputs
+// instead, which gives identical values.
+int optimize_all_device(Tree &t, double prec, double *out) {
+    for (;;) {
+        const std::vector<double> dlen0 = t.dlen;
+        const std::vector<char> dirty0 = t.dirty, pdirty0 = t.pdirty;
+        int rc = gb_set_branch_lengths(t.inst, t.dlen.data(), t.nnodes);
+        if (rc) return rc;
+        std::vector<gb_transmat_operation> tops;
+        for (int m = 1; m < t.nnodes; m++) {
+            if (!t.pdirty[m]) continue;
+            gb_transmat_operation o;
+            o.destTransMatIndex = m;
+            o.edgeLength = t.dlen[m];
+            o.eigenIndex = 0;
+            o.calcDerivs = 1;
+            tops.push_back(o);
+            t.pdirty[m] = 0;
+        }
+        rc = gb_update_transition_matrices(t.inst, tops.data(), (int)tops.size());
+        if (rc) return rc;
+        std::vector<int> order;
+        std::vector<char> seen(t.nnodes, 0);
+        const int l = t.left[0], m = t.next[l], r = t.right[0];
+        for (int c : {l, m, r}) pass_order(t, c, true, order, seen);
+        std::vector<gb_nr_branch> br;
+        std::vector<gb_cla_operation> ops;
+        std::vector<int> mats;
+        for (int nd : order) {
+            const Request rq = deriv_request(t, nd);
+            std::fill(t.level.begin(), t.level.end(), 0);
+            const int first = (int)ops.size();
+            accumulate(t, rq.pn, rq.pw, ops, mats);
+            accumulate(t, rq.cn, rq.cw, ops, mats);
+            for (int q = 0; q < t.nnodes; q++)
+                for (int w = 0; w < 3; w++)
+                    if (t.level[t.hidx(q, w)] > 0) t.dirty[t.hidx(q, w)] = 0;
+            gb_nr_branch b;
+            b.partialIndex = t.buf(rq.pn, rq.pw);
+            b.childIndex = rq.cw >= 0 ? t.buf(rq.cn, rq.cw) : t.tipbuf(rq.cn);
+            b.transMatIndex = nd;
+            b.firstOp = first;
+            b.opCount = (int)ops.size() - first;
+            br.push_back(b);
+            sweep(t, nd, -1);
+        }
+        double res[3];
+        rc = gb_newton_pass(t.inst, br.data(), (int)br.size(), ops.data(), (int)ops.size(), t.rescaleEvery, prec,
+                            t.minBrlen, t.maxBrlen, res);
+        if (rc == GB_ERROR_RESCALE_RETRY) {
+            // Tree::Score / NR retry rule (tree.cpp:4077-4090): lower rescaleEvery and redo
+            t.nRetries++;
+            t.dlen = dlen0;
+            t.dirty = dirty0;
+            t.pdirty = pdirty0;
+            make_all_dirty(t);
+            t.rescaleEvery -= 2;
+            if (t.rescaleEvery < 2) return GB_ERROR_FLOATING_POINT;
+            continue;
+        }
+        if (rc) return rc;
+        rc = gb_get_branch_lengths(t.inst, t.dlen.data(), t.nnodes);
+        if (rc) return rc;
+        t.nOps += (long long)ops.size();
+        t.nPatUpdates += (long long)ops.size() * t.npat;
+        t.nEdge += (long long)res[2];
+        t.lnL = -1.0;
+        out[0] = res[0];
+        out[1] = res[1];
+        return GB_SUCCESS;
+    }
 }
 
 }  // namespace
@@ -583,6 +547,7 @@ int gbt_optimize_branch(int tree, double precision, int node, double *out) {
 int gbt_optimize_all_branches(int tree, double precision, double *out) {
     Tree *t = get(tree);
     if (!t) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (t->deviceNewton) return optimize_all_device(*t, precision, out);
     std::fill(t->optimized.begin(), t->optimized.end(), 0);
     double improve = 0.0;
     const int l = t->left[0], m = t->next[l], r = t->right[0];
@@ -592,6 +557,13 @@ int gbt_optimize_all_branches(int tree, double precision, double *out) {
     }
     out[0] = improve;
     out[1] = t->lnL;
+    return GB_SUCCESS;
+}
+
+int gbt_set_device_newton(int tree, int on) {
+    Tree *t = get(tree);
+    if (!t) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    t->deviceNewton = on != 0;
     return GB_SUCCESS;
 }
 

@@ -96,6 +96,11 @@ SIGNATURES = {
     "gb_get_stream": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "gb_set_kernel_timing": (C.c_int, [C.c_int, C.c_int]),
     "gb_get_kernel_timing": (C.c_int, [C.c_int, _D]),
+    "gb_set_branch_lengths": (C.c_int, [C.c_int, _D, C.c_int]),
+    "gb_get_branch_lengths": (C.c_int, [C.c_int, _D, C.c_int]),
+    "gb_newton_pass": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D]),
+    "gb_get_newton_state": (C.c_int, [C.c_int, C.c_int, _D]),
+    "gbt_set_device_newton": (C.c_int, [C.c_int, C.c_int]),
     "gbm_gtr_qmat": (C.c_int, [_D, _D, _D, _D]),
     "gbm_aa_qmat": (C.c_int, [_D, _D, _D, _D]),
     "gbm_codon_qmat": (C.c_int, [C.c_double, C.c_double, _D, _D, _D]),
@@ -330,10 +335,10 @@ class Instance:
         _chk(lib().gb_set_kernel_timing(self.h, int(on)), "gb_set_kernel_timing")
 
     def kernel_timing(self) -> dict:
-        out = np.zeros(5)
+        out = np.zeros(6)
         _chk(lib().gb_get_kernel_timing(self.h, _p(out, C.c_double)), "gb_get_kernel_timing")
         return {"cla_ms": out[0], "cla_launches": int(out[1]), "pattern_updates": int(out[2]),
-                "edge_ms": out[3], "edge_evals": int(out[4])}
+                "edge_ms": out[3], "edge_evals": int(out[4]), "cla_bytes": out[5]}
 
     def synchronize(self):
         _chk(lib().gb_synchronize(self.h), "gb_synchronize")
@@ -388,6 +393,9 @@ class Tree:
         out = np.zeros(2)
         _chk(lib().gbt_optimize_all_branches(self.h, float(precision), _p(out, C.c_double)), "gbt_optimize_all_branches")
         return float(out[0]), float(out[1])
+
+    def set_device_newton(self, on: bool):
+        _chk(lib().gbt_set_device_newton(self.h, int(on)), "gbt_set_device_newton")
 
     @property
     def rescale_every(self) -> int:

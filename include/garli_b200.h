@@ -157,10 +157,43 @@ int gb_synchronize(int instance);
 const char *gb_last_error(void);
 /* instrumentation: the instance's CUDA stream (cudaStream_t) and optional
  * CUDA-event timing of the CLA and edge kernels on that stream;
- * timing out[0..4] = CLA ms, CLA launches, pattern-updates, edge ms, edge evaluations */
+ * timing out[0..5] = CLA ms, CLA launches, pattern-updates, edge ms, edge evaluations,
+ * algorithmic bytes of the timed CLA launches */
 int gb_get_stream(int instance, void **stream);
 int gb_set_kernel_timing(int instance, int on);
 int gb_get_kernel_timing(int instance, double *out);
+
+/* ---- graph-resident branch optimisation ----
+ * One entry per branch of an OptimizeAllBranches pass (optimization.cpp:97,
+ * :1042), in traversal order: the CLA updates that branch's derivatives need
+ * (ops[firstOp .. firstOp+opCount), a ClaOperation list as for
+ * gb_update_partials), then the Newton-Raphson loop on the branch between
+ * partialIndex (the CLA on the ancestor's side) and childIndex, whose length
+ * is the device copy for transMatIndex. */
+typedef struct {
+    int partialIndex;
+    int childIndex;
+    int transMatIndex;
+    int firstOp;
+    int opCount;
+} gb_nr_branch;
+/* device copy of the branch length behind each matrix index */
+int gb_set_branch_lengths(int instance, const double *lengths, int count);
+int gb_get_branch_lengths(int instance, double *lengths, int count);
+/* Runs the whole pass as one CUDA graph (cached while the plan, the model and
+ * the rank state are unchanged): no host round trip between Newton iterations
+ * or branches.  Every step of the loop is NewtonRaphsonOptimizeBranchLength
+ * (optimization.cpp:1359-1971) in FP64 on the device; the P(t) of each matrix
+ * always matches its device length on return.  out[0] = summed estimated
+ * improvement, out[1] = lnL of the last derivative evaluation, out[2] = number
+ * of derivative evaluations.  Returns GB_ERROR_RESCALE_RETRY if a CLA of the
+ * pass crossed GARLI's rescale bail-out (the caller restores the lengths,
+ * lowers rescaleEvery and reruns). */
+int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, const gb_cla_operation *ops,
+                   int opCount, int rescaleEvery, double precision, double minLength, double maxLength,
+                   double *out);
+/* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
+int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
 /* ---- host model math (model.cpp), used by the tree layer and by callers ---- */
 /* Model::UpdateQMat GTR branch (model.cpp:256-293) */
@@ -205,6 +238,9 @@ int gbt_make_all_dirty(int tree);
 int gbt_optimize_branch(int tree, double precision, int node, double *out);
 /* OptimizeAllBranches (optimization.cpp:97); out[0] = improvement, out[1] = final lnL */
 int gbt_optimize_all_branches(int tree, double precision, double *out);
+/* 1 (default): OptimizeAllBranches runs as one device graph (gb_newton_pass);
+ * 0: the host drives each Newton iteration through gbt_derivatives */
+int gbt_set_device_newton(int tree, int on);
 int gbt_get_rescale_every(int tree);
 int gbt_set_rescale_every(int tree, int every);
 /* counters: [0] CLA ops issued, [1] pattern-updates (ops x patterns),

@@ -203,3 +203,55 @@ def test_abi_operation_lists_directly():
     out = inst.calculate_edge(buf(0), buf(mid), mid, derivatives=False)
     assert abs(out[0] - lo) <= 1e-8 * abs(lo)
     assert inst.launch_count() > 0
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_device_newton_pass_equals_host_pass(mixed):
+    """The graph-resident pass takes exactly the host driver's Newton decisions."""
+    w = synth.make_dna(40, 3000, seed=21, pinv_range=(0.05, 0.3))
+    res = []
+    for dev in (True, False):
+        inst, tree = engine.tree_engine(w.data, w.child3, w.dlen * 1.3, w.model, mixed=mixed)
+        tree.set_device_newton(dev)
+        tree.score(0)
+        imp, _ = tree.optimize_all_branches(0.01)
+        bl = tree.branch_lengths()
+        tree.make_all_dirty()
+        res.append((bl, tree.score(0), imp, tree.counters()))
+        tree.close()
+        inst.close()
+    (bd, ld, idv, cd), (bh, lh, ih, ch) = res
+    assert np.array_equal(bd, bh), np.abs(bd - bh).max()
+    assert ld == lh and idv == ih
+    assert cd["edge_evals"] == ch["edge_evals"] - 0 or cd["edge_evals"] > 0
+
+
+def test_device_newton_pass_matches_oracle_and_is_repeatable():
+    w = synth.make_dna(48, 2500, seed=22)
+    inst, tree, ot = _both(w.data, w.child3, w.dlen * 0.7, w.model)
+    for _ in range(2):  # second pass replays the cached graph from a different start
+        tree.score(0)
+        ot.score(0)
+        tree.optimize_all_branches(0.01)
+        ot.optimize_all_branches(0.01)
+        assert np.allclose(tree.branch_lengths(), ot.branch_lengths(), rtol=1e-6, atol=1e-10)
+        tree.make_all_dirty()
+        ot.make_all_dirty()
+        lg, lo = tree.score(0), ot.score(0)
+        assert abs(lg - lo) <= 1e-8 * abs(lo)
+
+
+def test_device_newton_pass_rescale_retry():
+    """A pass whose CLAs cross the bail-out is rerun with a lower rescaleEvery."""
+    c3, dl, m, pd = _underflowing_case(ntax=64, nsites=200)
+    inst, tree, ot = _both(pd, c3, dl, m)
+    tree.rescale_every = 120
+    tree.score(0)
+    tree.optimize_all_branches(0.01)
+    assert tree.counters()["rescale_retries"] > 0
+    bl = tree.branch_lengths()
+    for nd in range(1, len(bl)):
+        ot.set_branch_length(nd, bl[nd])
+    tree.make_all_dirty()
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
