@@ -27,12 +27,39 @@ template <>
 __device__ __forceinline__ void cla_load<double>(const double *p, double v[4]) { ld4d(p, v); }
 template <>
 __device__ __forceinline__ void cla_load<float>(const float *p, double v[4]) { load4<float>(p, v); }
+// Stochastic rounding of a non-negative double to float: the lower or upper
+// float neighbour with probability given by the position between them, the
+// uniform variate being a hash of the value's address.  Unbiased and, unlike
+// round-to-nearest, uncorrelated between patterns: the CLAs of small subtrees
+// take few distinct values, and a deterministic rounding error of such a value
+// would be repeated in every pattern that shares it and add up coherently in
+// the lnL sum.  Deterministic (same address, same value -> same float).
+__device__ __forceinline__ float round_stochastic(double x, unsigned int key) {
+    const float lo = __double2float_rz(x);
+    const float hi = __int_as_float(__float_as_int(lo) + 1);
+    const double gap = (double)hi - (double)lo;
+    if (!(gap > 0.0) || !isfinite(hi)) return lo;
+    const double frac = (x - (double)lo) / gap;
+    unsigned int h = key * 0x9E3779B1u;
+    h ^= h >> 15;
+    h *= 0x85EBCA77u;
+    h ^= h >> 13;
+    h *= 0xC2B2AE3Du;
+    h ^= h >> 16;
+    const double u = (double)(h >> 8) * (1.0 / 16777216.0);
+    return u < frac ? hi : lo;
+}
+
 template <typename ST>
 __device__ __forceinline__ void cla_store(ST *p, const double v[4]);
 template <>
 __device__ __forceinline__ void cla_store<double>(double *p, const double v[4]) { st4d(p, v); }
 template <>
-__device__ __forceinline__ void cla_store<float>(float *p, const double v[4]) { store4<float>(p, v); }
+__device__ __forceinline__ void cla_store<float>(float *p, const double v[4]) {
+    const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(p) >> 2);
+    reinterpret_cast<float4 *>(p)[0] = make_float4(round_stochastic(v[0], key), round_stochastic(v[1], key + 1),
+                                                   round_stochastic(v[2], key + 2), round_stochastic(v[3], key + 3));
+}
 
 // (a*b + c*d) + (e*f + g*h): the unrolled 4-rate kernels (tree.cpp:7705-7779, :8319-8376)
 __device__ __forceinline__ double dot4_pair(const double *p, const double c[4]) {

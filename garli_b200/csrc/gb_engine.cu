@@ -21,6 +21,7 @@
 #include "gb_graph.cuh"
 #include "gb_newton_dna.cuh"
 #include "gb_nstate.cuh"
+#include "gb_persist.cuh"
 #include "gb_pmat.cuh"
 
 namespace gb {
@@ -36,6 +37,8 @@ struct Instance {
     int kpad = 0;        // patterns [0, kpad) stored in FP64 (internal order)
     int kpad_cap = 0;    // FP64 segment size the buffers are laid out for
     int nsm = 148;       // multiprocessors of the device
+    int nvb4 = 0;        // 4-state edge evaluations: blocks (= pattern partition) of every
+                         // edge kernel, equal to the persistent pass kernel's grid
     long long cla_bytes = 0;
     // host copies in the caller's pattern order and the internal permutation
     // (precision form: patterns with count >= kHeavyCount first, stored in FP64)
@@ -81,6 +84,16 @@ struct Instance {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_nodes = 0;
+    // persistent pass kernel (4 states): command queue and its scratch
+    PCmd *d_cmds = nullptr;
+    DevOp *d_pops = nullptr;
+    size_t cap_cmds = 0, cap_pops = 0;
+    GridSync *d_gsync = nullptr;
+    double *d_sums2 = nullptr;
+    unsigned long long pass_key = 0;
+    int use_persistent = 1;
+    unsigned long long *d_trace = nullptr;
+    int trace_cap = 0;
 
     long long mat_stride() const { return 3LL * R * S * S; }
     long long eig_stride() const { return (long long)S + 2LL * S * S; }
@@ -221,6 +234,15 @@ static int set_smem_attrs() {
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_pmats, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     return GB_SUCCESS;
+}
+
+static void *pass4_func(int R, bool garli) {
+#define GB_CASE(r) \
+    case r: return garli ? (void *)k_pass4<r, true> : (void *)k_pass4<r, false>;
+    switch (R) {
+        GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
+    }
+#undef GB_CASE
 }
 
 // grid of a 4-state CLA level: tiles x ops, about 16 resident blocks per SM in total
@@ -374,6 +396,11 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     if (rc) return fail(rc);
     if (cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(GB_ERROR_GENERAL);
     cudaDeviceGetAttribute(&I->nsm, cudaDevAttrMultiProcessorCount, resourceNumber);
+    if (stateCount == 4) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass4_func(categoryCount, !I->mixed), kThreads, 0);
+        I->nvb4 = std::min(kMaxScoreBlocks, std::max(1, per_sm) * I->nsm);
+    }
     const size_t P = I->npat_pad;
     const size_t cla_bytes = (size_t)I->nbuf * I->cla_bytes;
     struct A {
@@ -396,6 +423,8 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         {(void **)&I->d_site_lnl, P * sizeof(double)},
         {(void **)&I->d_len, (size_t)I->nmat * sizeof(double)},
         {(void **)&I->d_slots, (size_t)I->nmat * sizeof(NrSlot)},
+        {(void **)&I->d_gsync, sizeof(GridSync)},
+        {(void **)&I->d_sums2, (size_t)2 * 3 * kMaxScoreBlocks * sizeof(double)},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, a.n) != cudaSuccess) {
@@ -457,7 +486,8 @@ int gb_finalize_instance(int instance) {
     if (I->graph) cudaGraphDestroy(I->graph);
     void *ptrs[] = {I->d_partials, I->d_scalers, I->d_tips, I->d_counts, I->d_const, I->d_mats,
                     I->d_eigen, I->d_freqs, I->d_rates, I->d_rprobs, I->d_status, I->d_block_sums,
-                    I->d_result, I->d_site_lnl, I->d_len, I->d_slots};
+                    I->d_result, I->d_site_lnl, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
+                    I->d_cmds, I->d_pops};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     cudaFreeHost(I->h_result);
@@ -764,7 +794,7 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
     }
     int nblocks;
     if (I->S == 4) {
-        nblocks = std::min(kMaxScoreBlocks, (I->npat + kThreads - 1) / kThreads);
+        nblocks = I->nvb4;
         if (I->mixed) {
             if (D) launch_edge4<false, true>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
             else launch_edge4<false, false>(I->R, nblocks, I->stream, v, pb, cidx, op->transMatIndex, tip, 1);
@@ -1039,8 +1069,7 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
         ns_tp = ns_cla_tile(I, &ns_smem);
         ns_edge_tp = ns_edge_tile(I, &ns_edge_smem);
     }
-    const int nblocks = dna ? std::min(kMaxScoreBlocks, (I->npat + kThreads - 1) / kThreads)
-                            : std::min(kMaxScoreBlocks, (I->npat + ns_edge_tp - 1) / ns_edge_tp);
+    const int nblocks = dna ? I->nvb4 : std::min(kMaxScoreBlocks, (I->npat + ns_edge_tp - 1) / ns_edge_tp);
     const size_t pmat_smem = 3 * (size_t)I->R * I->S * sizeof(double);
     int rc;
     {
@@ -1126,6 +1155,80 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
     return GB_SUCCESS;
 }
 
+// Enqueue the pass as one cooperative launch of k_pass4 (4-state data).
+static int launch_persistent_pass(Instance *I, const gb_nr_branch *br, int nbr,
+                                  const std::vector<std::vector<std::vector<DevOp>>> &levels, int rescaleEvery,
+                                  NrParams prm, unsigned long long key) {
+    std::vector<PCmd> cmds;
+    std::vector<DevOp> flat;
+    for (int b = 0; b < nbr; b++) {
+        for (auto &lv : levels[b]) {
+            PCmd c;
+            c.type = kCmdLevel;
+            c.a = (int)flat.size();
+            c.b = (int)lv.size();
+            c.c = c.d = 0;
+            flat.insert(flat.end(), lv.begin(), lv.end());
+            cmds.push_back(c);
+        }
+        PCmd c;
+        c.type = kCmdNewton;
+        c.a = br[b].partialIndex - I->ntip;
+        const int tip = br[b].childIndex < I->ntip;
+        c.b = tip ? br[b].childIndex : br[b].childIndex - I->ntip;
+        c.c = tip;
+        c.d = br[b].transMatIndex;
+        cmds.push_back(c);
+    }
+    if (cmds.size() > I->cap_cmds) {
+        if (I->d_cmds) cudaFree(I->d_cmds);
+        I->cap_cmds = cmds.size() * 2;
+        GB_CUDA(cudaMalloc(&I->d_cmds, I->cap_cmds * sizeof(PCmd)));
+        I->pass_key = 0;
+    }
+    if (flat.size() > I->cap_pops || !I->d_pops) {
+        if (I->d_pops) cudaFree(I->d_pops);
+        I->cap_pops = std::max<size_t>(16, flat.size() * 2);
+        GB_CUDA(cudaMalloc(&I->d_pops, I->cap_pops * sizeof(DevOp)));
+        I->pass_key = 0;
+    }
+    if (key != I->pass_key) {
+        GB_CUDA(cudaMemcpyAsync(I->d_cmds, cmds.data(), cmds.size() * sizeof(PCmd), cudaMemcpyHostToDevice, I->stream));
+        if (!flat.empty())
+            GB_CUDA(cudaMemcpyAsync(I->d_pops, flat.data(), flat.size() * sizeof(DevOp), cudaMemcpyHostToDevice, I->stream));
+        I->pass_key = key;
+    }
+    GB_CUDA(cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream));
+    View v = make_view(I);
+    v.rescale_every = rescaleEvery;
+    PassArgs A;
+    A.cmds = I->d_cmds;
+    A.ncmd = (int)cmds.size();
+    A.ops = I->d_pops;
+    A.prm = prm;
+    A.lengths = I->d_len;
+    A.eig = I->d_eigen;
+    A.rates = I->d_rates;
+    A.slots = I->d_slots;
+    A.gs = I->d_gsync;
+    A.sums2 = I->d_sums2;
+    A.nvb = I->nvb4;
+    A.trace = I->d_trace;
+    A.trace_cap = I->trace_cap;
+    void *func = pass4_func(I->R, !I->mixed);
+    int per_sm = 0;
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
+    if (per_sm < 1) {
+        g_last_error = "persistent pass kernel cannot be resident";
+        return GB_ERROR_NO_RESOURCE;
+    }
+    dim3 grid(std::min(per_sm * I->nsm, I->nvb4));
+    void *args[] = {&v, &A};
+    GB_CUDA(cudaLaunchCooperativeKernel(func, grid, dim3(kThreads), args, 0, I->stream));
+    I->launches += 1;
+    return GB_SUCCESS;
+}
+
 }  // namespace gb
 
 extern "C" {
@@ -1182,7 +1285,16 @@ int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, 
     key = fnv(key, &rescaleEvery, sizeof(int));
     key = fnv(key, &prm, sizeof(prm));
     key = fnv(key, &I->version, sizeof(I->version));
-    if (key != I->graph_key || !I->graph_exec) {
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, I->device);
+    const bool persistent = I->S == 4 && I->use_persistent && coop;
+    if (persistent) {
+        int rc = launch_persistent_pass(I, branches, branchCount, levels, rescaleEvery, prm, key);
+        if (rc) {
+            I->rank = rank_before;
+            return rc;
+        }
+    } else if (key != I->graph_key || !I->graph_exec) {
         int rc = build_pass_graph(I, branches, branchCount, levels, rescaleEvery, prm);
         if (rc) {
             I->rank = rank_before;
@@ -1191,8 +1303,10 @@ int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, 
         }
         I->graph_key = key;
     }
-    GB_CUDA(cudaGraphLaunch(I->graph_exec, I->stream));
-    I->launches += I->graph_nodes;
+    if (!persistent) {
+        GB_CUDA(cudaGraphLaunch(I->graph_exec, I->stream));
+        I->launches += I->graph_nodes;
+    }
     std::vector<NrSlot> slots(I->nmat);
     GB_CUDA(cudaMemcpyAsync(slots.data(), I->d_slots, I->nmat * sizeof(NrSlot), cudaMemcpyDeviceToHost, I->stream));
     GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
@@ -1211,12 +1325,53 @@ int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, 
         out[2] = (double)evals;
     }
     I->site_valid = true;
+    if (*I->h_status & kStatusBarrierTimeout) {
+        GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        g_last_error = "persistent pass: grid barrier wait exceeded its bound";
+        return GB_ERROR_GENERAL;
+    }
     if (*I->h_status & kStatusRescaleRetry) {
         GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
         GB_CUDA(cudaStreamSynchronize(I->stream));
         I->graph_key = 0;
         return GB_ERROR_RESCALE_RETRY;
     }
+    return GB_SUCCESS;
+}
+
+// Instrumentation: record up to `capacity` phase timestamps of the persistent
+// pass kernel (block 0); capacity 0 switches it off.
+int gb_set_pass_trace(int instance, int capacity) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    cudaSetDevice(I->device);
+    if (I->d_trace) cudaFree(I->d_trace);
+    I->d_trace = nullptr;
+    I->trace_cap = 0;
+    if (capacity > 0) {
+        GB_CUDA(cudaMalloc(&I->d_trace, (size_t)capacity * sizeof(unsigned long long)));
+        GB_CUDA(cudaMemset(I->d_trace, 0, (size_t)capacity * sizeof(unsigned long long)));
+        I->trace_cap = capacity;
+    }
+    return GB_SUCCESS;
+}
+
+int gb_get_pass_trace(int instance, unsigned long long *out, int count) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!I->d_trace || count > I->trace_cap) return GB_ERROR_OUT_OF_RANGE;
+    cudaSetDevice(I->device);
+    GB_CUDA(cudaMemcpy(out, I->d_trace, (size_t)count * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return GB_SUCCESS;
+}
+
+// 1 (default): 4-state passes run as one cooperative persistent kernel;
+// 0: as a CUDA graph with a conditional WHILE node per branch
+int gb_set_pass_mode(int instance, int persistent) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->use_persistent = persistent != 0;
     return GB_SUCCESS;
 }
 

@@ -100,6 +100,9 @@ SIGNATURES = {
     "gb_get_branch_lengths": (C.c_int, [C.c_int, _D, C.c_int]),
     "gb_newton_pass": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D]),
     "gb_get_newton_state": (C.c_int, [C.c_int, C.c_int, _D]),
+    "gb_set_pass_mode": (C.c_int, [C.c_int, C.c_int]),
+    "gb_set_pass_trace": (C.c_int, [C.c_int, C.c_int]),
+    "gb_get_pass_trace": (C.c_int, [C.c_int, C.POINTER(C.c_ulonglong), C.c_int]),
     "gbt_set_device_newton": (C.c_int, [C.c_int, C.c_int]),
     "gbm_gtr_qmat": (C.c_int, [_D, _D, _D, _D]),
     "gbm_aa_qmat": (C.c_int, [_D, _D, _D, _D]),
@@ -342,6 +345,9 @@ class Instance:
 
     def synchronize(self):
         _chk(lib().gb_synchronize(self.h), "gb_synchronize")
+
+    def set_pass_mode(self, persistent: bool):
+        _chk(lib().gb_set_pass_mode(self.h, int(persistent)), "gb_set_pass_mode")
 
 
 class Tree:

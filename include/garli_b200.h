@@ -192,6 +192,13 @@ int gb_get_branch_lengths(int instance, double *lengths, int count);
 int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, const gb_cla_operation *ops,
                    int opCount, int rescaleEvery, double precision, double minLength, double maxLength,
                    double *out);
+/* 1 (default): 4-state passes run as one cooperative persistent kernel over a
+ * device command queue; 0: as a CUDA graph with a conditional WHILE node per branch */
+int gb_set_pass_mode(int instance, int persistent);
+/* instrumentation: phase timestamps of the persistent pass kernel, each
+ * (phase code << 56) | %globaltimer ns; capacity 0 switches recording off */
+int gb_set_pass_trace(int instance, int capacity);
+int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 /* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
 int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
