@@ -12,8 +12,8 @@
 //                decisions everywhere, one barrier per iteration.
 // Commands are separated by grid barriers.  Data written inside the launch by
 // other blocks is read through L2 (ld.global.cg), never the incoherent L1 /
-// read-only path.  Every barrier wait is bounded: a block that waits longer
-// than kSpinLimit sets an error bit and the whole launch winds down.
+// read-only path.  Every barrier wait is bounded (poll count and wall time): a
+// block that gives up sets an error bit and the whole launch winds down.
 #pragma once
 #include "gb_dna.cuh"
 #include "gb_graph.cuh"
@@ -23,7 +23,8 @@ namespace gb {
 
 enum CmdType : int { kCmdLevel = 1, kCmdNewton = 2 };
 enum : int { kStatusBarrierTimeout = 4 };
-constexpr long long kSpinLimit = 1LL << 25;
+constexpr long long kSpinLimit = 1LL << 26;
+constexpr unsigned long long kBarrierNs = 4000000000ULL;  // 4 s
 
 struct PCmd {
     int type;
@@ -49,42 +50,53 @@ __device__ __forceinline__ void red_release_gpu(unsigned int *p, unsigned int v)
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Sense-counting grid barrier for a cooperative launch (all blocks resident):
-// acquire/release atomics at GPU scope, the CTA's earlier writes ordered by a
-// fence before arrival.  The wait is bounded; a block that gives up sets an
-// error bit and every block then returns false from this and later barriers.
-__device__ __forceinline__ bool grid_barrier(GridSync *gs, int *status) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned int g = ld_acquire_gpu(&gs->gen);
-        __threadfence();
-        const unsigned int arrived = atom_add_acq_rel_gpu(&gs->count, 1u) + 1u;
-        int ok = 1;
-        if (arrived == gridDim.x) {
-            gs->count = 0;
-            red_release_gpu(&gs->gen, 1u);
-        } else {
-            long long spins = 0;
-            while (ld_acquire_gpu(&gs->gen) == g) {
-                if (++spins > kSpinLimit) {
-                    atomicOr(status, kStatusBarrierTimeout);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        if (*(volatile int *)status & kStatusBarrierTimeout) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// Sense-counting grid barrier for a cooperative launch (all blocks resident):
+// acquire/release atomics at GPU scope, the CTA's earlier writes ordered by a
+// fence before arrival.  The wait is bounded twice (kSpinLimit polls and
+// kBarrierNs of %globaltimer); a block that gives up sets an error bit, and a
+// waiting block that sees the bit stops waiting, so every block returns false
+// from this and later barriers and the launch winds down promptly.
+__device__ __forceinline__ bool grid_barrier(GridSync *gs, int *status) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = (*(volatile int *)status & kStatusBarrierTimeout) ? 0 : 1;
+        if (ok) {
+            const unsigned int g = ld_acquire_gpu(&gs->gen);
+            __threadfence();
+            const unsigned int arrived = atom_add_acq_rel_gpu(&gs->count, 1u) + 1u;
+            if (arrived == gridDim.x) {
+                gs->count = 0;
+                red_release_gpu(&gs->gen, 1u);
+            } else {
+                const unsigned long long t0 = global_ns();
+                long long spins = 0;
+                while (ld_acquire_gpu(&gs->gen) == g) {
+                    if ((++spins & 255) == 0) {
+                        if (*(volatile int *)status & kStatusBarrierTimeout) {
+                            ok = 0;
+                            break;
+                        }
+                        if (spins > kSpinLimit || global_ns() - t0 > kBarrierNs) {
+                            atomicOr(status, kStatusBarrierTimeout);
+                            ok = 0;
+                            break;
+                        }
+                    }
+                }
+            }
+            if (*(volatile int *)status & kStatusBarrierTimeout) ok = 0;
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
 }
 
 // L2-coherent loads for data other blocks of the same launch may have written
