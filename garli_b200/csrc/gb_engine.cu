@@ -327,6 +327,9 @@ static void resolve_timing(Instance *I) {
 
 using namespace gb;
 
+// Lets the library's other translation units report through gb_last_error().
+void gb_internal_set_last_error(const std::string &msg) { g_last_error = msg; }
+
 extern "C" {
 
 const char *gb_last_error(void) { return g_last_error.c_str(); }

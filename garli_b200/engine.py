@@ -104,6 +104,8 @@ SIGNATURES = {
     "gb_set_pass_trace": (C.c_int, [C.c_int, C.c_int]),
     "gb_get_pass_trace": (C.c_int, [C.c_int, C.POINTER(C.c_ulonglong), C.c_int]),
     "gbt_set_device_newton": (C.c_int, [C.c_int, C.c_int]),
+    "gb_edge_loglik_static": (C.c_int, [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 10 + [C.c_double, C.c_int, C.c_int,
+                                                                                          C.c_void_p, C.c_void_p]),
     "gbm_gtr_qmat": (C.c_int, [_D, _D, _D, _D]),
     "gbm_aa_qmat": (C.c_int, [_D, _D, _D, _D]),
     "gbm_codon_qmat": (C.c_int, [C.c_double, C.c_double, _D, _D, _D]),

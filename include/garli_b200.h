@@ -202,6 +202,38 @@ int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 /* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
 int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
+/* ---- edge evaluation without device allocation ----
+ * No counterpart in the reference: GARLI's beagle build lets beagle allocate.
+ * For callers that cannot call cudaMalloc -- code running while a CUDA graph
+ * is captured, or a plugin inside a host that owns every device allocation
+ * through its own pool -- this evaluates lnL (and d1, d2) across one branch
+ * of 4-state data held entirely in the caller's device arrays, with the plain
+ * FP64 form's per-site arithmetic (GARLI's e-based integer scalers).  It
+ * allocates nothing: its per-block partial sums live in a fixed 96 KiB array
+ * that the library keeps on every GPU that loads it, until the process exits.
+ *   partial, child ........ FP64 CLAs, layout [pattern][category][4]
+ *   childTipCodes ......... instead of child (pass child = NULL): 4-bit masks per pattern
+ *   partialScalers, childScalers: int per pattern (childScalers only with a CLA child)
+ *   matrices .............. [P | dP | d2P], each [category][from][to] (dP, d2P only
+ *                           read when derivatives != 0)
+ *   stateFrequencies[4], categoryWeights[categoryCount], patternCounts[patternCount],
+ *   constantStates ........ 4-bit mask of a constant pattern, -1 otherwise (read when hasPinv)
+ *   out ................... device array of 3 doubles: lnL, d1, d2 (d1 = d2 = 0 without derivatives)
+ * All pointers are device pointers on device resourceNumber.  The call is
+ * asynchronous on `stream` (a cudaStream_t; NULL = the default stream).
+ * patternCount above GB_STATIC_EDGE_MAX_PATTERNS is rejected with
+ * GB_ERROR_OUT_OF_RANGE.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress): make that first call before any
+ * stream capture.  Every call shares the one array, so calls that overlap on
+ * the GPU (unordered streams) race; calls ordered on one stream do not. */
+#define GB_STATIC_EDGE_MAX_PATTERNS 4194304
+int gb_edge_loglik_static(int resourceNumber, int categoryCount, int patternCount, const double *partial,
+                          const int *partialScalers, const double *child, const int *childScalers,
+                          const unsigned char *childTipCodes, const double *matrices,
+                          const double *stateFrequencies, const double *categoryWeights,
+                          const int *patternCounts, const int *constantStates, double pinv, int hasPinv,
+                          int derivatives, void *stream, double *out);
+
 /* ---- host model math (model.cpp), used by the tree layer and by callers ---- */
 /* Model::UpdateQMat GTR branch (model.cpp:256-293) */
 int gbm_gtr_qmat(const double *rel6, const double *pi4, double *Q, double *blenMult);
