@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/garli_b200.h"
+#include "gb_batch.cuh"
 #include "gb_common.cuh"
 #include "gb_dna.cuh"
 #include "gb_graph.cuh"
@@ -94,6 +95,19 @@ struct Instance {
     int use_persistent = 1;
     unsigned long long *d_trace = nullptr;
     int trace_cap = 0;
+    // batched candidate pass (gb_batch_newton): queue, results and scratch
+    BCmd *d_bcmds = nullptr;
+    DevOp *d_bops = nullptr;
+    BEntry *d_bentries = nullptr;
+    BSlot *d_bslots = nullptr;
+    double *d_chunk_sums = nullptr;
+    int *d_active = nullptr;  // 2 x cap_bentries, then 2 counters
+    size_t cap_bcmds = 0, cap_bops = 0, cap_bentries = 0, cap_bslots = 0, cap_chunk = 0, cap_active = 0;
+    int batch_tiles = 0, batch_chunks = 0;  // 0: autotune on the next call
+    cudaGraph_t bgraph = nullptr;
+    cudaGraphExec_t bgraph_exec = nullptr;
+    unsigned long long bgraph_key = 0;
+    int use_batch_graph = 1;
 
     long long mat_stride() const { return 3LL * R * S * S; }
     long long eig_stride() const { return (long long)S + 2LL * S * S; }
@@ -490,7 +504,10 @@ int gb_finalize_instance(int instance) {
     void *ptrs[] = {I->d_partials, I->d_scalers, I->d_tips, I->d_counts, I->d_const, I->d_mats,
                     I->d_eigen, I->d_freqs, I->d_rates, I->d_rprobs, I->d_status, I->d_block_sums,
                     I->d_result, I->d_site_lnl, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
-                    I->d_cmds, I->d_pops};
+                    I->d_cmds, I->d_pops, I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots,
+                    I->d_chunk_sums, I->d_active};
+    if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
+    if (I->bgraph) cudaGraphDestroy(I->bgraph);
     for (void *p : ptrs)
         if (p) cudaFree(p);
     cudaFreeHost(I->h_result);
@@ -1392,6 +1409,348 @@ int gb_get_newton_state(int instance, int matrixIndex, double *out) {
     out[3] = sl.d1;
     out[4] = sl.d2;
     out[5] = sl.evals;
+    return GB_SUCCESS;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched candidate pass (gb_batch_newton): the host builds the command queue
+// of k_batch4 (gb_batch.cuh) -- dependency levels of every candidate's CLA
+// updates, then per step the step's CLA updates and one lockstep Newton
+// command over all candidates, then a final score -- uploads it when it
+// changes, and launches it cooperatively (captured once in a CUDA graph).
+// ---------------------------------------------------------------------------
+namespace gb {
+
+static void *batch4_func(int R, bool garli) {
+#define GB_CASE(r) \
+    case r: return garli ? (void *)k_batch4<r, true> : (void *)k_batch4<r, false>;
+    switch (R) {
+        GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
+    }
+#undef GB_CASE
+}
+
+template <typename T>
+static int grow_device(T **p, size_t *cap, size_t need) {
+    if (*p && need <= *cap) return GB_SUCCESS;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    const size_t c = std::max<size_t>(16, need + need / 2);
+    GB_CUDA(cudaMalloc((void **)p, c * sizeof(T)));
+    *cap = c;
+    return GB_SUCCESS;
+}
+
+struct BatchPlan {
+    std::vector<BCmd> cmds;
+    std::vector<DevOp> ops;
+    std::vector<BEntry> entries;
+    int max_entries = 0;
+    unsigned long long key = 0;
+};
+
+// Enqueue one batched pass on the instance stream (no synchronisation).
+static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery, int tiles, int chunks,
+                         bool use_graph) {
+    void *func = batch4_func(I->R, !I->mixed);
+    int per_sm = 0;
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
+    if (per_sm < 1) {
+        g_last_error = "batched pass kernel cannot be resident";
+        return GB_ERROR_NO_RESOURCE;
+    }
+    View v = make_view(I);
+    v.rescale_every = rescaleEvery;
+    BatchArgs A;
+    A.cmds = I->d_bcmds;
+    A.ncmd = (int)P.cmds.size();
+    A.ops = I->d_bops;
+    A.entries = I->d_bentries;
+    A.slots = I->d_bslots;
+    A.prm = prm;
+    A.lengths = I->d_len;
+    A.eig = I->d_eigen;
+    A.rates = I->d_rates;
+    A.chunk_sums = I->d_chunk_sums;
+    A.active = I->d_active;
+    A.nactive = I->d_active + 2 * P.max_entries;
+    A.max_entries = P.max_entries;
+    A.gs = I->d_gsync;
+    A.tiles_per_item = tiles;
+    A.chunks_per_item = chunks;
+    void *args[] = {&v, &A};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(per_sm * I->nsm);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = I->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const unsigned long long gkey = P.key ^ ((unsigned long long)tiles << 40) ^ ((unsigned long long)chunks << 48) ^
+                                    ((unsigned long long)rescaleEvery << 56);
+    if (use_graph && I->use_batch_graph) {
+        if (gkey != I->bgraph_key || !I->bgraph_exec) {
+            if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
+            if (I->bgraph) cudaGraphDestroy(I->bgraph);
+            I->bgraph_exec = nullptr;
+            I->bgraph = nullptr;
+            I->bgraph_key = 0;
+            bool ok = cudaStreamBeginCapture(I->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                const bool m = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream) == cudaSuccess;
+                const bool k = m && cudaLaunchKernelExC(&cfg, func, args) == cudaSuccess;
+                cudaGraph_t g = nullptr;
+                const bool e = cudaStreamEndCapture(I->stream, &g) == cudaSuccess;
+                ok = m && k && e && g;
+                if (ok && cudaGraphInstantiate(&I->bgraph_exec, g, 0) != cudaSuccess) ok = false;
+                if (ok) {
+                    I->bgraph = g;
+                    I->bgraph_key = gkey;
+                } else {
+                    if (g) cudaGraphDestroy(g);
+                    I->bgraph_exec = nullptr;
+                    I->use_batch_graph = 0;  // capture unsupported here: launch directly from now on
+                }
+            } else {
+                I->use_batch_graph = 0;
+            }
+            cudaGetLastError();
+        }
+        if (I->bgraph_exec) {
+            GB_CUDA(cudaGraphLaunch(I->bgraph_exec, I->stream));
+            I->launches += 1;
+            return GB_SUCCESS;
+        }
+    }
+    GB_CUDA(cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream));
+    GB_CUDA(cudaLaunchKernelExC(&cfg, func, args));
+    I->launches += 1;
+    return GB_SUCCESS;
+}
+
+// Picks (CLA tiles, edge chunks) per work item by timing whole passes on the
+// real batch.  Every trial starts from the same lengths and matrices (saved
+// and restored on the device); the results do not depend on the choice.
+static int autotune_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery) {
+    const size_t len_bytes = (size_t)I->nmat * sizeof(double);
+    const size_t mat_bytes = (size_t)I->nmat * I->mat_stride() * sizeof(double);
+    double *save = nullptr;
+    GB_CUDA(cudaMalloc((void **)&save, len_bytes + mat_bytes));
+    GB_CUDA(cudaMemcpyAsync(save, I->d_len, len_bytes, cudaMemcpyDeviceToDevice, I->stream));
+    GB_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(save) + len_bytes, I->d_mats, mat_bytes,
+                            cudaMemcpyDeviceToDevice, I->stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int tiles_c[] = {1, 2, 4, 8};
+    const int chunks_c[] = {1, 2, 4};
+    float best = 1e30f;
+    int bt = 1, bc = 1, rc = GB_SUCCESS;
+    for (int t : tiles_c) {
+        for (int c : chunks_c) {
+            for (int rep = 0; rep < 2 && rc == GB_SUCCESS; rep++) {  // first run warms up
+                cudaMemcpyAsync(I->d_len, save, len_bytes, cudaMemcpyDeviceToDevice, I->stream);
+                cudaMemcpyAsync(I->d_mats, reinterpret_cast<char *>(save) + len_bytes, mat_bytes,
+                                cudaMemcpyDeviceToDevice, I->stream);
+                cudaEventRecord(e0, I->stream);
+                rc = enqueue_batch(I, P, prm, rescaleEvery, t, c, false);
+                cudaEventRecord(e1, I->stream);
+                if (cudaStreamSynchronize(I->stream) != cudaSuccess) rc = GB_ERROR_GENERAL;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep == 1 && ms < best) {
+                    best = ms;
+                    bt = t;
+                    bc = c;
+                }
+            }
+        }
+    }
+    cudaMemcpyAsync(I->d_len, save, len_bytes, cudaMemcpyDeviceToDevice, I->stream);
+    cudaMemcpyAsync(I->d_mats, reinterpret_cast<char *>(save) + len_bytes, mat_bytes, cudaMemcpyDeviceToDevice,
+                    I->stream);
+    cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream);
+    cudaStreamSynchronize(I->stream);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(save);
+    if (rc) return rc;
+    I->batch_tiles = bt;
+    I->batch_chunks = bc;
+    return GB_SUCCESS;
+}
+
+}  // namespace gb
+
+extern "C" {
+
+int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, const gb_cla_operation *stepOps,
+                    int stepOpCount, const gb_batch_step *steps, int candidateCount, int stepsPerCandidate,
+                    int rescaleEvery, double precision, double minLength, double maxLength, double *out) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (I->S != 4) {
+        g_last_error = "gb_batch_newton: 4-state data only";
+        return GB_ERROR_NO_IMPLEMENTATION;
+    }
+    if (opCount < 0 || stepOpCount < 0 || candidateCount < 1 || stepsPerCandidate < 1 || !(precision > 0.0) ||
+        !(minLength > 0.0) || !(maxLength > minLength) || !steps || !out)
+        return GB_ERROR_OUT_OF_RANGE;
+    const int nC = candidateCount, K = stepsPerCandidate;
+    for (int i = 0; i < nC * K; i++) {
+        const gb_batch_step &s = steps[i];
+        if (s.claOp < -1 || s.claOp >= stepOpCount || s.transMatIndex < 0 || s.transMatIndex >= I->nmat ||
+            s.partialIndex < I->ntip || s.partialIndex >= I->ntip + I->nbuf || s.childIndex < 0 ||
+            s.childIndex >= I->ntip + I->nbuf)
+            return GB_ERROR_OUT_OF_RANGE;
+    }
+    cudaSetDevice(I->device);
+    const std::vector<int> rank_before = I->rank;
+    BatchPlan P;
+    std::vector<std::vector<DevOp>> levels;
+    int rc = prepare_ops(I, ops, opCount, rescaleEvery, levels);
+    unsigned long long key = 1469598103934665603ULL;
+    auto add_level = [&](const std::vector<DevOp> &lv) {
+        BCmd c;
+        c.type = kBLevel;
+        c.a = (int)P.ops.size();
+        c.b = (int)lv.size();
+        P.ops.insert(P.ops.end(), lv.begin(), lv.end());
+        P.cmds.push_back(c);
+        key = fnv(key, lv.data(), sizeof(DevOp) * lv.size());
+    };
+    if (rc == GB_SUCCESS)
+        for (auto &lv : levels) add_level(lv);
+    for (int k = 0; k < K && rc == GB_SUCCESS; k++) {
+        std::vector<gb_cla_operation> sops;
+        for (int c = 0; c < nC; c++)
+            if (steps[c * K + k].claOp >= 0) {
+                gb_cla_operation o = stepOps[steps[c * K + k].claOp];
+                o.opDepLevel = 1;  // the ops of one step are independent of each other
+                sops.push_back(o);
+            }
+        std::vector<std::vector<DevOp>> sl;
+        rc = prepare_ops(I, sops.data(), (int)sops.size(), rescaleEvery, sl);
+        if (rc) break;
+        for (auto &lv : sl) add_level(lv);
+        BCmd nc;
+        nc.type = kBNewton;
+        nc.a = (int)P.entries.size();
+        nc.b = nC;
+        for (int c = 0; c < nC; c++) {
+            const gb_batch_step &s = steps[c * K + k];
+            BEntry e;
+            e.pbuf = s.partialIndex - I->ntip;
+            e.tip = s.childIndex < I->ntip;
+            e.cbuf = e.tip ? s.childIndex : s.childIndex - I->ntip;
+            e.mat = s.transMatIndex;
+            P.entries.push_back(e);
+        }
+        P.cmds.push_back(nc);
+    }
+    if (rc) {
+        I->rank = rank_before;
+        return rc;
+    }
+    BCmd fs;  // lnL of every candidate at its optimised lengths
+    fs.type = kBScore;
+    fs.a = (K - 1) * nC;
+    fs.b = nC;
+    P.cmds.push_back(fs);
+    P.max_entries = nC;
+    key = fnv(key, P.entries.data(), sizeof(BEntry) * P.entries.size());
+    key = fnv(key, P.cmds.data(), sizeof(BCmd) * P.cmds.size());
+    key = fnv(key, &I->version, sizeof(I->version));
+    P.key = key;
+    const int nchunks = (I->npat + kChunk - 1) / kChunk;
+    bool realloc = false;
+    {
+        const void *before[] = {I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots, I->d_chunk_sums, I->d_active};
+        if ((rc = grow_device(&I->d_bcmds, &I->cap_bcmds, P.cmds.size())) ||
+            (rc = grow_device(&I->d_bops, &I->cap_bops, std::max<size_t>(1, P.ops.size()))) ||
+            (rc = grow_device(&I->d_bentries, &I->cap_bentries, P.entries.size())) ||
+            (rc = grow_device(&I->d_bslots, &I->cap_bslots, P.entries.size())) ||
+            (rc = grow_device(&I->d_chunk_sums, &I->cap_chunk, (size_t)nC * nchunks * 3)) ||
+            (rc = grow_device(&I->d_active, &I->cap_active, (size_t)2 * nC + 2))) {
+            I->rank = rank_before;
+            return rc;
+        }
+        const void *after[] = {I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots, I->d_chunk_sums, I->d_active};
+        for (int i = 0; i < 6; i++) realloc = realloc || before[i] != after[i];
+    }
+    if (realloc) I->bgraph_key = 0;
+    GB_CUDA(cudaMemcpyAsync(I->d_bcmds, P.cmds.data(), P.cmds.size() * sizeof(BCmd), cudaMemcpyHostToDevice,
+                            I->stream));
+    if (!P.ops.empty())
+        GB_CUDA(cudaMemcpyAsync(I->d_bops, P.ops.data(), P.ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice,
+                                I->stream));
+    GB_CUDA(cudaMemcpyAsync(I->d_bentries, P.entries.data(), P.entries.size() * sizeof(BEntry),
+                            cudaMemcpyHostToDevice, I->stream));
+    NrParams prm{precision, minLength, maxLength};
+    if (I->batch_tiles == 0 || I->batch_chunks == 0) {
+        if ((rc = autotune_batch(I, P, prm, rescaleEvery))) {
+            I->rank = rank_before;
+            return rc;
+        }
+    }
+    if ((rc = enqueue_batch(I, P, prm, rescaleEvery, I->batch_tiles, I->batch_chunks, true))) {
+        I->rank = rank_before;
+        return rc;
+    }
+    std::vector<BSlot> slots(P.entries.size());
+    GB_CUDA(cudaMemcpyAsync(slots.data(), I->d_bslots, slots.size() * sizeof(BSlot), cudaMemcpyDeviceToHost,
+                            I->stream));
+    GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    for (int c = 0; c < nC; c++) {
+        double imp = 0.0;
+        long long ev = 0;
+        for (int k = 0; k < K; k++) {
+            imp += slots[k * nC + c].st.totalEstImprove;
+            ev += slots[k * nC + c].evals;
+        }
+        out[4 * c] = slots[c].first_lnL;
+        out[4 * c + 1] = slots[(K - 1) * nC + c].score;
+        out[4 * c + 2] = imp;
+        out[4 * c + 3] = (double)ev;
+    }
+    const int st = *I->h_status;
+    if (st) {
+        GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+    }
+    if (st & kStatusBarrierTimeout) {
+        g_last_error = "batched pass: grid barrier wait exceeded its bound";
+        return GB_ERROR_GENERAL;
+    }
+    if (st & kStatusRescaleRetry) return GB_ERROR_RESCALE_RETRY;
+    return GB_SUCCESS;
+}
+
+// Work-item sizes of the batched pass: CLA tiles (64 patterns at 4 categories)
+// and edge chunks (256 patterns) per work item; 0, 0 = autotune on the next call.
+int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (tilesPerItem < 0 || tilesPerItem > 64 || chunksPerItem < 0 || chunksPerItem > 64) return GB_ERROR_OUT_OF_RANGE;
+    I->batch_tiles = tilesPerItem;
+    I->batch_chunks = chunksPerItem;
+    I->bgraph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_get_batch_tuning(int instance, int *out3) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    out3[0] = I->batch_tiles;
+    out3[1] = I->batch_chunks;
+    out3[2] = I->use_batch_graph && I->bgraph_exec ? 1 : 0;
     return GB_SUCCESS;
 }
 

@@ -104,6 +104,15 @@ SIGNATURES = {
     "gb_set_pass_trace": (C.c_int, [C.c_int, C.c_int]),
     "gb_get_pass_trace": (C.c_int, [C.c_int, C.POINTER(C.c_ulonglong), C.c_int]),
     "gbt_set_device_newton": (C.c_int, [C.c_int, C.c_int]),
+    "gb_batch_newton": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                  C.c_int, C.c_double, C.c_double, C.c_double, _D]),
+    "gb_set_batch_tuning": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "gb_get_batch_tuning": (C.c_int, [C.c_int, _I]),
+    "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),
+    "gbp_destroy": (C.c_int, [C.c_int]),
+    "gbp_invalidate": (C.c_int, [C.c_int]),
+    "gbp_score_candidates": (C.c_int, [C.c_int, C.c_int, _I, _D, _I, C.c_double, C.c_int, _D, _D]),
+    "gbp_get_counters": (C.c_int, [C.c_int, _LL]),
     "gb_edge_loglik_static": (C.c_int, [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 10 + [C.c_double, C.c_int, C.c_int,
                                                                                           C.c_void_p, C.c_void_p]),
     "gbm_gtr_qmat": (C.c_int, [_D, _D, _D, _D]),
@@ -432,3 +441,62 @@ def tree_engine(pd, child3, dlen, model: Model, device=0, mixed=False):
     tree = Tree(inst, child3, dlen)
     tree.set_model(model)
     return inst, tree
+
+
+# ---------------------------------------------------------------- GA population
+class Population:
+    """A GA generation's candidates scored on one instance (gbp_* ABI).
+
+    ``base`` is the parent tree (child3, dlen); candidates are trees on the same
+    node numbers with the connector node of their move (synth.ga_candidates)."""
+
+    def __init__(self, inst: Instance, child3: np.ndarray, dlen: np.ndarray, nmat: int):
+        self.inst = inst
+        self.nnodes = child3.shape[0]
+        c3 = _i32(np.asarray(child3).reshape(-1))
+        h = lib().gbp_create(inst.h, (self.nnodes + 2) // 2, _p(c3, C.c_int), _p(_f64(dlen), C.c_double), nmat)
+        _chk(h, "gbp_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", -1) >= 0:
+            lib().gbp_destroy(self.h)
+            self.h = -1
+
+    def score(self, child3s, dlens, connectors, precision=0.01, sequential=False):
+        """Per candidate: (rescore lnL, optimised lnL, improvement, evaluations) and
+        the optimised lengths of connector.left, connector, connector.right."""
+        n = len(connectors)
+        c3 = _i32(np.asarray(child3s).reshape(-1))
+        dl = _f64(np.asarray(dlens).reshape(-1))
+        cn = _i32(connectors)
+        out = np.zeros((n, 4))
+        lens = np.zeros((n, 3))
+        _chk(lib().gbp_score_candidates(self.h, n, _p(c3, C.c_int), _p(dl, C.c_double), _p(cn, C.c_int),
+                                        float(precision), int(sequential), _p(out, C.c_double),
+                                        _p(lens, C.c_double)), "gbp_score_candidates")
+        return out, lens
+
+    def counters(self) -> dict:
+        out = np.zeros(4, dtype=np.int64)
+        _chk(lib().gbp_get_counters(self.h, out.ctypes.data_as(_LL)), "gbp_get_counters")
+        return {"cla_ops": int(out[0]), "pattern_updates": int(out[1]), "edge_evals": int(out[2]),
+                "base_cla_ops": int(out[3])}
+
+    def tuning(self) -> dict:
+        out = np.zeros(3, dtype=np.int32)
+        _chk(lib().gb_get_batch_tuning(self.inst.h, _p(out, C.c_int)), "gb_get_batch_tuning")
+        return {"tiles_per_item": int(out[0]), "chunks_per_item": int(out[1]), "cuda_graph": bool(out[2])}
+
+
+def population_engine(pd, child3, dlen, model: Model, ncand: int, device=0, mixed=True, extra_bufs_per_cand=40):
+    """Instance + Population sized for ``ncand`` candidates of a base tree."""
+    ntax = pd.ntax
+    nnodes = 2 * ntax - 2
+    nbuf = 3 * (ntax - 2) + ncand * (extra_bufs_per_cand + 1)
+    nmat = nnodes + ncand * 8
+    inst = Instance(ntax, nbuf, pd.nstates, pd.npat, model.ncat, nmat, device=device, mixed=mixed)
+    inst.set_data(pd)
+    inst.set_model(model)
+    pop = Population(inst, child3, dlen, nmat)
+    return inst, pop

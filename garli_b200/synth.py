@@ -191,3 +191,134 @@ def codon(seed=3, ntax=32, ncodons=5_000) -> Workload:
     m = codon_model(rng)
     st = simulate(child3, dlen, m, ncodons, rng)
     return Workload(f"codon_gy94_{ntax}x{ncodons}", child3, dlen, m, compress(st, 61))
+
+
+# ---------------------------------------------------------------- GA candidates
+MIN_BRLEN = 1e-8  # defs.h:106
+
+
+def _adjacency(child3, dlen):
+    nb = {}
+    ln = {}
+    for v in range(child3.shape[0]):
+        for c in child3[v]:
+            if c >= 0:
+                c = int(c)
+                nb.setdefault(v, []).append(c)
+                nb.setdefault(c, []).append(v)
+                ln[(min(v, c), max(v, c))] = float(dlen[c])
+    return nb, ln
+
+
+def _layout(nb, ln, nnodes, root=0):
+    """GARLI layout of an unrooted tree rooted at ``root`` (keeps node numbers;
+    neighbour order is kept as stored in ``nb``)."""
+    child3 = -np.ones((nnodes, 3), dtype=np.int32)
+    dlen = np.zeros(nnodes)
+    stack = [(root, -1)]
+    while stack:
+        v, par = stack.pop()
+        kids = [c for c in nb[v] if c != par]
+        if par >= 0:
+            dlen[v] = ln[(min(v, par), max(v, par))]
+        if v == root:
+            child3[v] = kids
+        elif kids:
+            child3[v] = [kids[0], -1, kids[1]]
+        for c in kids:
+            stack.append((c, v))
+    return child3, dlen
+
+
+def spr_move(child3, dlen, rng, radius):
+    """One SPR move of Tree::SPRMutate (tree.cpp:3148-3248) on a GARLI-layout tree.
+
+    A random non-root internal node P (the connector) and one of its children
+    ``cut`` are chosen; P is pruned (its two other neighbours a, b joined, the
+    joined branch keeping the sum of both lengths) and regrafted into a branch
+    at edge distance ``radius`` from the joined one (radius 1 = an NNI), both
+    halves of that branch getting max(len / 2, min_brlen).  Returns the new
+    (child3, dlen) on the same node numbers (root 0 stays the trifurcating
+    root) and the connector P, whose left child is ``cut`` and right child the
+    lower node of the broken branch, as in GARLI."""
+    nnodes = child3.shape[0]
+    ntax = (nnodes + 2) // 2
+    nb, ln = _adjacency(child3, dlen)
+    anc = {int(c): v for v in range(nnodes) for c in child3[v] if c >= 0}
+    for _ in range(1000):
+        P = int(rng.integers(ntax + 1, nnodes))
+        cut = int(child3[P][0] if rng.random() < 0.5 else child3[P][2])
+        a, b = [c for c in nb[P] if c != cut]
+        # nodes of the cut subtree (on cut's side of P)
+        sub, st = set(), [cut]
+        while st:
+            v = st.pop()
+            sub.add(v)
+            st += [c for c in nb[v] if c != P and c not in sub]
+        # edges of the remaining tree with the joined edge (a, b), by BFS over edges
+        nb2 = {v: [c for c in nb[v] if c != P] for v in nb if v != P and v not in sub}
+        nb2[a].append(b)
+        nb2[b].append(a)
+        dist = {(min(a, b), max(a, b)): 0}
+        frontier = [(a, b)]
+        while frontier:
+            nxt = []
+            for (x, y) in frontier:
+                d = dist[(min(x, y), max(x, y))]
+                for end in (x, y):
+                    for z in nb2[end]:
+                        e = (min(end, z), max(end, z))
+                        if e not in dist:
+                            dist[e] = d + 1
+                            nxt.append(e)
+            frontier = nxt
+        cands = [e for e, d in dist.items() if d == radius]
+        if not cands:
+            continue
+        u, w = cands[int(rng.integers(len(cands)))]
+        break
+    else:
+        raise RuntimeError("no SPR move of that radius")
+    # prune P
+    lab = ln.pop((min(a, P), max(a, P)))
+    lbp = ln.pop((min(b, P), max(b, P)))
+    nb[a] = [b if c == P else c for c in nb[a]]
+    nb[b] = [a if c == P else c for c in nb[b]]
+    ln[(min(a, b), max(a, b))] = lab + lbp
+    # regraft on (u, w): P between them
+    t = ln.pop((min(u, w), max(u, w)))
+    half = max(t * 0.5, MIN_BRLEN)
+    nb[u] = [P if c == w else c for c in nb[u]]
+    nb[w] = [P if c == u else c for c in nb[w]]
+    ln[(min(u, P), max(u, P))] = half
+    ln[(min(w, P), max(w, P))] = half
+    # P's neighbours: its future parent (the one of u, w nearer the root) first, then cut, broken
+    new_nb = dict(nb)
+    new_nb[P] = [u, w, cut]
+    c3, dl = _layout(new_nb, ln, nnodes)
+    par = next(v for v in range(nnodes) if P in c3[v])
+    broken = w if par == u else u
+    c3[P] = [cut, -1, broken]
+    return c3, dl, P
+
+
+def ga_candidates(child3, dlen, count, seed, radius_range=(1, 8)):
+    """``count`` candidates of one generation, each the base tree after one SPR
+    move with radius ~ Uniform{radius_range} (NNI = radius 1)."""
+    rng = np.random.default_rng(seed)
+    nnodes = child3.shape[0]
+    c3s = np.zeros((count, nnodes, 3), dtype=np.int32)
+    dls = np.zeros((count, nnodes))
+    conn = np.zeros(count, dtype=np.int32)
+    for i in range(count):
+        r = int(rng.integers(radius_range[0], radius_range[1] + 1))
+        c3s[i], dls[i], conn[i] = spr_move(child3, dlen, rng, r)
+    return c3s, dls, conn
+
+
+def batch_workload(seed=4, ntax=64, nsites=50_000, ncand=256):
+    """The GA-population workload: a Yule base tree, GTR+G4, its alignment, and
+    ``ncand`` SPR/NNI candidates of it (radius ~ U{1..8})."""
+    w = make_dna(ntax, nsites, seed, name=f"ga_batch_dna_gtr_g4_{ntax}x{nsites}_{ncand}cand")
+    c3s, dls, conn = ga_candidates(w.child3, w.dlen, ncand, seed + 1000)
+    return w, c3s, dls, conn

@@ -202,6 +202,65 @@ int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 /* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
 int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
+/* ---- batched candidate scoring and branch optimisation (4 states) ----
+ * A GA generation's candidates (population.cpp:4532-4589: each mutated
+ * individual is rescored, tree.cpp:4003, and the branches around its move are
+ * optimised, optimization.cpp:882-884 -> NewtonRaphsonOptimizeBranchLength,
+ * :1359-1971) run as one persistent kernel over a device command queue.
+ * ops[0..opCount): every candidate's dirty CLA updates, levelled by opDepLevel
+ * (uneven counts per candidate are fine; buffers may be shared read-only).
+ * steps[c * stepsPerCandidate + k]: step k of candidate c -- optionally the CLA
+ * update stepOps[claOp] (the partial of this step, which may read lengths
+ * optimised at earlier steps), then Newton-Raphson on the branch between
+ * partialIndex and childIndex whose length is the device copy for
+ * transMatIndex (gb_set_branch_lengths).  All candidates take step k in
+ * lockstep; the matrices hold the optimised P(t) on return.
+ * out[4c .. 4c+3] = lnL at the starting lengths (the candidate's rescore),
+ * lnL at the optimised lengths, summed estimated improvement, derivative
+ * evaluations.  Work-item sizes are autotuned on the first call. */
+typedef struct {
+    int claOp;
+    int partialIndex;
+    int childIndex;
+    int transMatIndex;
+} gb_batch_step;
+int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, const gb_cla_operation *stepOps,
+                    int stepOpCount, const gb_batch_step *steps, int candidateCount, int stepsPerCandidate,
+                    int rescaleEvery, double precision, double minLength, double maxLength, double *out);
+/* work-item sizes: CLA tiles (64 patterns at 4 categories) and edge chunks
+ * (256 patterns) per CTA work item; 0, 0 = autotune on the next call */
+int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem);
+/* out[0..2] = tiles per item, chunks per item, 1 if the pass replays a CUDA graph */
+int gb_get_batch_tuning(int instance, int *out3);
+
+/* ---- population layer: a GA generation's candidates on one instance ----
+ * A C++ restatement of how GARLI scores the candidates of a generation: each
+ * is the base tree after one SPR/NNI move (Tree::SPRMutate, tree.cpp:3148-3248)
+ * and shares every unchanged CLA with it (copy-on-write holders,
+ * clamanager.h); it is rescored and the three branches at the move's
+ * connector nd are optimised in GARLI's order nd->left, nd, nd->right
+ * (optimization.cpp:882-884).  CLAs are identified by content (subtree,
+ * tips and branch lengths), so only changed ones are recomputed.
+ * gbp_create: base tree in GARLI layout; matrixCount <= the instance's
+ * matrixBufferCount matrix slots are used.  The instance must hold the model
+ * (gb_set_eigen_decomposition etc.) and the tips. */
+int gbp_create(int instance, int ntax, const int *child3, const double *dlen, int matrixCount);
+int gbp_destroy(int pop);
+/* the instance's model changed: recompute the base tree's CLAs on the next call */
+int gbp_invalidate(int pop);
+/* candidate c: child3s[c*nnodes*3 ...], dlens[c*nnodes ...] (GARLI layout, the
+ * base tree's node numbers), connectors[c] = the move's connector node nd.
+ * sequential = 0: all candidates in one gb_batch_newton pass; 1: GARLI's
+ * per-tree path, one candidate after another with a host Newton loop.
+ * out[4c .. 4c+3] as gb_batch_newton; lengthsOut[3c .. 3c+2] = optimised
+ * lengths of nd->left, nd, nd->right. */
+int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const double *dlens,
+                         const int *connectors, double precision, int sequential, double *out,
+                         double *lengthsOut);
+/* last call: [0] CLA updates, [1] pattern-updates, [2] derivative evaluations;
+ * [3] base-tree CLA updates since creation */
+int gbp_get_counters(int pop, long long *out4);
+
 /* ---- edge evaluation without device allocation ----
  * No counterpart in the reference: GARLI's beagle build lets beagle allocate.
  * For callers that cannot call cudaMalloc -- code running while a CUDA graph
