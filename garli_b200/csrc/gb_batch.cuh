@@ -63,7 +63,11 @@ struct BatchArgs {
     GridSync *gs;
     int tiles_per_item;   // CLA work item: this many 64-pattern tiles
     int chunks_per_item;  // edge work item: this many 256-pattern chunks
+    unsigned long long *trace;  // optional phase timestamps of block 0: (code << 56) | ns
+    int trace_cap;
 };
+
+enum BatchTrace : int { kBtLevel = 1, kBtNewton, kBtSweepDone, kBtStepDone, kBtCmdDone };
 
 constexpr int kChunk = kThreads;  // patterns per edge chunk (one per thread)
 
@@ -156,8 +160,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4(View v, BatchArgs A) {
     const int warps_per_block = blockDim.x / 32;
     const int gwarp = blockIdx.x * warps_per_block + threadIdx.x / 32;
     const int nwarps = gridDim.x * warps_per_block;
+    int ntr = 0;
+    auto mark = [&](int code, int na) {
+        if (A.trace && blockIdx.x == 0 && threadIdx.x == 0 && ntr < A.trace_cap)
+            A.trace[ntr++] = ((unsigned long long)code << 56) | ((unsigned long long)(na & 0xffff) << 40) |
+                             (global_ns() & ((1ULL << 40) - 1));
+    };
     for (int ci = 0; ci < A.ncmd; ci++) {
         const BCmd cmd = A.cmds[ci];
+        mark(cmd.type == kBLevel ? kBtLevel : kBtNewton, cmd.b);
         if (cmd.type == kBLevel) {
             const int tpi = A.tiles_per_item;
             const int items_per_op = (ntiles + tpi - 1) / tpi;
@@ -185,6 +196,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4(View v, BatchArgs A) {
                 }
             }
             if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtCmdDone, 0);
             continue;
         }
         // Newton / score over entries [a, a+n)
@@ -227,6 +239,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4(View v, BatchArgs A) {
                                                   A.chunk_sums + (long long)k * nchunks * 3);
             }
             if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtSweepDone, na);
             if (blockIdx.x == 0 && threadIdx.x == 0) A.nactive[cur] = 0;  // every block has read it
             // (B) one warp per active entry: reduce, Newton step, new P
             const int nxt = cur ^ 1;
@@ -261,10 +274,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4(View v, BatchArgs A) {
                 }
             }
             if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtStepDone, na);
             cur = nxt;
         }
         // every block has left the loop before the next command resets the counters
         if (!grid_barrier(A.gs, v.status)) return;
+        mark(kBtCmdDone, 0);
     }
 }
 

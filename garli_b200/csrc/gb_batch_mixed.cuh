@@ -1,0 +1,595 @@
+// gb_batch_mixed.cuh -- the precision form's batched candidate kernel.
+//
+// Same command queue as k_batch4 (gb_batch.cuh), laid out for throughput:
+//   kBLevel : CLA updates with one lane per (pattern, category), the op's P
+//             blocks in padded shared memory, FP64 fused arithmetic, the
+//             pattern's power-of-two normalisation by a shuffle max, FP32
+//             stores with unbiased stochastic rounding (exact, no division);
+//             the child loads of kU tiles are issued before any arithmetic.
+//   kBCoef  : for every candidate's step, the spectral coefficients of the
+//             branch it optimises.  With P_r(t) = U diag(exp(s_rk t)) U^-1,
+//             s_rk = lambda_k rate_r / (1 - pinv),
+//               L_p(t) = sum_rk A[p,r,k] exp(s_rk t) (+ the +I term), with
+//               A[p,r,k] = w_r (sum_i pi_i W[p,r,i] U[i,k]) (sum_j U^-1[k,j] V[p,r,j]),
+//             where W = (P_o1 V_o1) o (P_o2 V_o2) is the partial on the
+//             connector's side, formed in FP64 registers and never stored,
+//             and V the CLA (or tip) across the branch.  One lane per
+//             (pattern, category), loads first as in kBLevel.  A is FP64,
+//             laid out [slot][r*4+k][pattern]; the site's scale exponent is
+//             m_o1 + m_o2 + m_V.
+//   kBNewton: Newton-Raphson in lockstep; an iteration reads only A:
+//             L = sum A e, dL/dt = sum A s e, d2L/dt2 = sum A s^2 e with the
+//             per-candidate tables e, s e, s^2 e recomputed in FP64 after
+//             every step.  A chunk = 256 patterns summed by one warp (8 per
+//             lane, then a shuffle tree) -- no block barrier; the candidate's
+//             chunk sums are reduced by one warp in a fixed order.
+//   kBScore : the same sweep at the optimised lengths.
+// lnL, d1, d2 accumulate in FP64; the Newton step and P(t) are FP64.
+#pragma once
+#include "gb_batch.cuh"
+
+namespace gb {
+
+enum : int { kBCoef = 4 };
+
+// a step in the precision form: the two other sides (buffer or tip, matrix;
+// m2 < 0: side 1 is the partial itself, no matrix) and the side across the branch
+struct MEntry {
+    int b1, t1, m1;
+    int b2, t2, m2;
+    int bk, tk, mk;
+};
+
+struct MixedArgs {
+    const BCmd *cmds;
+    int ncmd;
+    const DevOp *ops;
+    const MEntry *entries;
+    BSlot *slots;
+    NrParams prm;
+    double *lengths;
+    const double *eig;    // lambda (scaled), U, U^-1
+    const double *rates;
+    double *coef;         // max_entries x 16R... [slot][R*4][npat_pad]
+    int *cscale;          // max_entries x npat_pad
+    double *etab;         // max_entries x 3 x R*4
+    double *chunk_sums;   // max_entries x nchunks x 3
+    int *active;
+    int *nactive;
+    int max_entries;
+    GridSync *gs;
+    int tiles_per_item;   // CLA / coefficient work item: this many tiles of 256/G patterns
+    int chunks_per_item;  // sweep work item: this many 256-pattern chunks per warp
+    unsigned long long *trace;
+    int trace_cap;
+};
+
+// 2^k as a double, k in [-1022, 1023]
+__device__ __forceinline__ double pow2d(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// Unbiased stochastic rounding of a non-negative finite double to float: the
+// upper neighbour with probability (x - lo) / ulp, the uniform variate a hash
+// of `key`.  The gap between the float neighbours is a power of two, so the
+// fraction is an exact scaling (no division).
+__device__ __forceinline__ float round_stochastic_exact(double x, unsigned int key) {
+    const float lo = __double2float_rz(x);
+    const float hi = __int_as_float(__float_as_int(lo) + 1);
+    if (!isfinite(hi)) return lo;
+    const double gap = (double)hi - (double)lo;  // exact: a power of two
+    const int ge = (int)((__double_as_longlong(gap) >> 52) & 0x7ff) - 1023;
+    const double frac = (x - (double)lo) * pow2d(-ge);
+    unsigned int h = key * 0x9E3779B1u;
+    h ^= h >> 15;
+    h *= 0x85EBCA77u;
+    h ^= h >> 13;
+    h *= 0xC2B2AE3Du;
+    h ^= h >> 16;
+    const double u = (double)(h >> 8) * (1.0 / 16777216.0);
+    return u < frac ? hi : lo;
+}
+
+// Power-of-two normalisation of one pattern-category slice d[4] (the max over
+// the pattern's G lanes) and its store: FP64 segment as is, FP32 segment with
+// stochastic rounding.  All G lanes of the pattern must call this together.
+template <int R>
+__device__ __forceinline__ void cla_finish_m(const View &v, int dest, int p, int r, bool act, double d[4], int m) {
+    constexpr int G = Lanes<R>::G;
+    double mx = act ? fmax(fmax(d[0], d[1]), fmax(d[2], d[3])) : 0.0;
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (!act) return;
+    int e = 0;
+    if (mx > 0.0) e = max(-1000, min(1000, ilogb(mx)));
+    const double sc = pow2d(-e);
+#pragma unroll
+    for (int k = 0; k < 4; k++) d[k] *= sc;
+    if (p < v.kpad) {
+        st4d(cla_ptr<double>(v, dest, p, R * 4) + r * 4, d);
+    } else {
+        float *q = cla_ptr<float>(v, dest, p, R * 4) + r * 4;
+        const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(q) >> 2);
+        reinterpret_cast<float4 *>(q)[0] =
+            make_float4(round_stochastic_exact(d[0], key), round_stochastic_exact(d[1], key + 1),
+                        round_stochastic_exact(d[2], key + 2), round_stochastic_exact(d[3], key + 3));
+    }
+    if (r == 0) v.scalers[(long long)dest * v.npat_pad + p] = m - e;
+}
+
+// (P c) for the 4 states of one category (P: that category's 4x4 block), FP64 fused
+__device__ __forceinline__ void pvec(const double *P, const double c[4], double out[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) out[i] = fma(P[i * 4 + 3], c[3], fma(P[i * 4 + 2], c[2], fma(P[i * 4 + 1], c[1], P[i * 4] * c[0])));
+}
+__device__ __forceinline__ void pvec_tip(const double *P, int code, double out[4]) {
+    code &= 15;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            if (code & (1 << b)) s += P[i * 4 + b];
+        out[i] = (code == 15 || code == 0) ? 1.0 : s;
+    }
+}
+
+// CLA update of tiles [t0, t1) of one op; lane = category r of pattern
+// tile * PPB + threadIdx.x / G; PL, PR = the category's P blocks in shared
+// memory.  FP32 tiles run in groups of kU with every child load of the group
+// issued before any arithmetic (memory-level parallelism); the small FP64
+// segment runs tile by tile.
+constexpr int kU = 2;
+template <int R>
+__device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, const double *PL, const double *PR,
+                                            int t0, int t1, int r, bool lane_ok) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    const int pl = threadIdx.x / G;
+    int tile = t0;
+    // FP64 segment (kpad is a multiple of 128 patterns, i.e. of whole tiles)
+    for (; tile < t1 && tile * PPB < v.kpad; tile++) {
+        const int p = tile * PPB + pl;
+        const bool act = lane_ok && p < v.npat;
+        double d[4] = {0, 0, 0, 0}, x[4], y[4];
+        int m = 0;
+        if (act) {
+            if (op.kind == kTipTip) {
+                pvec_tip(PL, v.tips[(long long)op.c1 * v.npat_pad + p], x);
+                pvec_tip(PR, v.tips[(long long)op.c2 * v.npat_pad + p], y);
+            } else {
+                double a[4];
+                ld4d_cg(cla_ptr<double>(v, op.c1, p, R * 4) + r * 4, a);
+                pvec(PL, a, x);
+                m = __ldcg(v.scalers + (long long)op.c1 * v.npat_pad + p);
+                if (op.kind == kIntInt) {
+                    double b[4];
+                    ld4d_cg(cla_ptr<double>(v, op.c2, p, R * 4) + r * 4, b);
+                    pvec(PR, b, y);
+                    m += __ldcg(v.scalers + (long long)op.c2 * v.npat_pad + p);
+                } else {
+                    pvec_tip(PR, v.tips[(long long)op.c2 * v.npat_pad + p], y);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
+        }
+        cla_finish_m<R>(v, op.dest, p, r, act, d, m);
+    }
+    // FP32 segment, kU tiles at a time
+    for (; tile < t1; tile += kU) {
+        float4 A4[kU], B4[kU];
+        int M[kU];
+        unsigned char T1[kU], T2[kU];
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int p = (tile + u) * PPB + pl;
+            const bool act = lane_ok && tile + u < t1 && p < v.npat;
+            A4[u] = B4[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            M[u] = 0;
+            T1[u] = T2[u] = 15;
+            if (!act) continue;
+            if (op.kind == kTipTip) {
+                T1[u] = v.tips[(long long)op.c1 * v.npat_pad + p];
+                T2[u] = v.tips[(long long)op.c2 * v.npat_pad + p];
+                continue;
+            }
+            A4[u] = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, op.c1, p, R * 4) + r * 4));
+            M[u] = __ldcg(v.scalers + (long long)op.c1 * v.npat_pad + p);
+            if (op.kind == kIntInt) {
+                B4[u] = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, op.c2, p, R * 4) + r * 4));
+                M[u] += __ldcg(v.scalers + (long long)op.c2 * v.npat_pad + p);
+            } else {
+                T2[u] = v.tips[(long long)op.c2 * v.npat_pad + p];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int p = (tile + u) * PPB + pl;
+            const bool act = lane_ok && tile + u < t1 && p < v.npat;
+            double d[4] = {0, 0, 0, 0}, x[4], y[4];
+            if (act) {
+                if (op.kind == kTipTip) {
+                    pvec_tip(PL, T1[u], x);
+                } else {
+                    const double a[4] = {A4[u].x, A4[u].y, A4[u].z, A4[u].w};
+                    pvec(PL, a, x);
+                }
+                if (op.kind == kIntInt) {
+                    const double b[4] = {B4[u].x, B4[u].y, B4[u].z, B4[u].w};
+                    pvec(PR, b, y);
+                } else {
+                    pvec_tip(PR, T2[u], y);
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
+            }
+            cla_finish_m<R>(v, op.dest, p, r, act, d, M[u]);
+        }
+    }
+}
+
+// One side of a coefficient entry for lane category r at pattern p: the raw
+// child slice (FP32 segment) or tip code, loaded before any arithmetic.
+struct SideRaw {
+    float4 c;
+    int code, scale;
+};
+template <int R>
+__device__ __forceinline__ void side_load(const View &v, int b, int tip, int p, int r, SideRaw &s) {
+    s.c = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.code = 15;
+    s.scale = 0;
+    if (b < 0) return;
+    if (tip) {
+        s.code = v.tips[(long long)b * v.npat_pad + p];
+        return;
+    }
+    s.c = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, b, p, R * 4) + r * 4));
+    s.scale = __ldcg(v.scalers + (long long)b * v.npat_pad + p);
+}
+// the side's vector (P_s V_s) (or V_s itself when it has no matrix), FP64
+__device__ __forceinline__ void side_vec(const double c[4], int code, int tip, const double *P, double out[4]) {
+    if (tip) {
+        if (P) {
+            pvec_tip(P, code, out);
+        } else {
+            code &= 15;
+#pragma unroll
+            for (int k = 0; k < 4; k++) out[k] = (code == 15 || code == 0 || (code >> k) & 1) ? 1.0 : 0.0;
+        }
+    } else if (P) {
+        pvec(P, c, out);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) out[k] = c[k];
+    }
+}
+
+// Coefficients A[r][k], k = 0..3, of category r at pattern p from the three
+// side vectors; stored to the entry's slot.
+template <int R>
+__device__ __forceinline__ void coef_store(const View &v, const MixedArgs &A, int slot, int p, int r, const double x[4],
+                                           const double y[4], const double z[4], int scale, const double *sU,
+                                           const double *sUi) {
+    double w[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = x[i] * y[i] * v.freqs[i];
+    const double rp = v.rate_probs[r];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double a_k = fma(w[3], sU[12 + k], fma(w[2], sU[8 + k], fma(w[1], sU[4 + k], w[0] * sU[k])));
+        const double b_k = fma(sUi[k * 4 + 3], z[3], fma(sUi[k * 4 + 2], z[2], fma(sUi[k * 4 + 1], z[1], sUi[k * 4] * z[0])));
+        A.coef[((long long)slot * R * 4 + r * 4 + k) * v.npat_pad + p] = rp * a_k * b_k;
+    }
+    if (r == 0) A.cscale[(long long)slot * v.npat_pad + p] = scale;
+}
+
+// Coefficient pass of tiles [t0, t1) of one entry; lane = category r of
+// pattern tile * PPB + threadIdx.x / G.  P1, P2 = the sides' P blocks of
+// category r (null: no matrix), sU / sUi = U and U^-1 in shared memory.
+template <int R>
+__device__ __forceinline__ void coef_tiles_m(const View &v, const MixedArgs &A, const MEntry &en, const double *P1,
+                                             const double *P2, const double *sU, const double *sUi, int slot, int t0,
+                                             int t1, int r, bool lane_ok) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    const int pl = threadIdx.x / G;
+    int tile = t0;
+    for (; tile < t1 && tile * PPB < v.kpad; tile++) {  // FP64 segment
+        const int p = tile * PPB + pl;
+        if (!(lane_ok && p < v.npat)) continue;
+        int scale = 0;
+        double x[4], y[4] = {1, 1, 1, 1}, z[4], c[4] = {0, 0, 0, 0};
+        int code = 15;
+        if (en.t1) code = v.tips[(long long)en.b1 * v.npat_pad + p];
+        else {
+            ld4d_cg(cla_ptr<double>(v, en.b1, p, R * 4) + r * 4, c);
+            scale += __ldcg(v.scalers + (long long)en.b1 * v.npat_pad + p);
+        }
+        side_vec(c, code, en.t1, P1, x);
+        if (en.b2 >= 0) {
+            code = 15;
+            if (en.t2) code = v.tips[(long long)en.b2 * v.npat_pad + p];
+            else {
+                ld4d_cg(cla_ptr<double>(v, en.b2, p, R * 4) + r * 4, c);
+                scale += __ldcg(v.scalers + (long long)en.b2 * v.npat_pad + p);
+            }
+            side_vec(c, code, en.t2, P2, y);
+        }
+        code = 15;
+        if (en.tk) code = v.tips[(long long)en.bk * v.npat_pad + p];
+        else {
+            ld4d_cg(cla_ptr<double>(v, en.bk, p, R * 4) + r * 4, c);
+            scale += __ldcg(v.scalers + (long long)en.bk * v.npat_pad + p);
+        }
+        side_vec(c, code, en.tk, nullptr, z);
+        coef_store<R>(v, A, slot, p, r, x, y, z, scale, sU, sUi);
+    }
+    for (; tile < t1; tile += kU) {  // FP32 segment, loads of kU tiles first
+        SideRaw S1[kU], S2[kU], SK[kU];
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int p = (tile + u) * PPB + pl;
+            const bool act = lane_ok && tile + u < t1 && p < v.npat;
+            side_load<R>(v, act ? en.b1 : -1, en.t1, p, r, S1[u]);
+            side_load<R>(v, act ? en.b2 : -1, en.t2, p, r, S2[u]);
+            side_load<R>(v, act ? en.bk : -1, en.tk, p, r, SK[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int p = (tile + u) * PPB + pl;
+            if (!(lane_ok && tile + u < t1 && p < v.npat)) continue;
+            double x[4], y[4] = {1, 1, 1, 1}, z[4];
+            const double c1[4] = {S1[u].c.x, S1[u].c.y, S1[u].c.z, S1[u].c.w};
+            side_vec(c1, S1[u].code, en.t1, P1, x);
+            if (en.b2 >= 0) {
+                const double c2[4] = {S2[u].c.x, S2[u].c.y, S2[u].c.z, S2[u].c.w};
+                side_vec(c2, S2[u].code, en.t2, P2, y);
+            }
+            const double ck[4] = {SK[u].c.x, SK[u].c.y, SK[u].c.z, SK[u].c.w};
+            side_vec(ck, SK[u].code, en.tk, nullptr, z);
+            coef_store<R>(v, A, slot, p, r, x, y, z, S1[u].scale + S2[u].scale + SK[u].scale, sU, sUi);
+        }
+    }
+}
+
+// e, s e, s^2 e of all (r, k) at length t, by one warp, into etab[3][R*4]
+template <int R>
+__device__ __forceinline__ void etab_warp(const double *eig, const double *rates, double pinv, int has_pinv, double t,
+                                          double *etab) {
+    const int lane = threadIdx.x & 31;
+    for (int idx = lane; idx < R * 4; idx += 32) {
+        const int r = idx / 4, k = idx % 4;
+        double s = __ldcg(eig + k) * __ldcg(rates + r);
+        if (has_pinv) s = s / (1.0 - pinv);
+        const double e = exp(s * t);
+        etab[idx] = e;
+        etab[R * 4 + idx] = s * e;
+        etab[2 * R * 4 + idx] = s * s * e;
+    }
+}
+
+// One warp sums a 256-pattern chunk of one entry: lnL, d1, d2 into sums[0..2].
+template <int R>
+__device__ __forceinline__ void sweep_chunk(const View &v, const MixedArgs &A, int slot, const double *E, int c,
+                                            double *sums) {
+    const int lane = threadIdx.x & 31;
+    double aL = 0.0, a1 = 0.0, a2 = 0.0;
+    const double *cf = A.coef + (long long)slot * R * 4 * v.npat_pad;
+    const int *cs = A.cscale + (long long)slot * v.npat_pad;
+#pragma unroll 2
+    for (int j = 0; j < 8; j++) {
+        const int p = c * 256 + j * 32 + lane;
+        if (p >= v.npat) break;
+        double L = 0.0, D1 = 0.0, D2 = 0.0;
+#pragma unroll
+        for (int q = 0; q < R * 4; q++) {
+            const double a = __ldcg(cf + (long long)q * v.npat_pad + p);
+            L = fma(a, E[q], L);
+            D1 = fma(a, E[R * 4 + q], D1);
+            D2 = fma(a, E[2 * R * 4 + q], D2);
+        }
+        const int m = __ldcg(cs + p);
+        const int cb = v.const_states[p];
+        if (v.has_pinv && cb >= 0) {
+            double btot = 0.0;
+#pragma unroll
+            for (int s = 0; s < 4; s++)
+                if (cb & (1 << s)) btot += v.freqs[s];
+            L += ldexp(v.pinv * btot, m);
+        }
+        const double cnt = (double)v.counts[p];
+        const double inv = 1.0 / L;
+        const double sd1 = D1 * inv;
+        aL = fma(cnt, log(L) - (double)m * 0.69314718055994530941723212145818, aL);
+        a1 = fma(cnt, sd1, a1);
+        a2 = fma(cnt, fma(D2, inv, -sd1 * sd1), a2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        aL += __shfl_xor_sync(0xffffffffu, aL, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+        sums[0] = aL;
+        sums[1] = a1;
+        sums[2] = a2;
+    }
+}
+
+// P blocks of the current CLA op: [matrix][category][4x4 + 1 pad] (the pad
+// keeps the categories of a warp in different banks)
+constexpr int kPStride = 17;
+
+template <int R>
+__global__ void __launch_bounds__(kThreads, 3) k_batch4m(View v, MixedArgs A) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;           // patterns per CLA tile
+    __shared__ double sE[8][3 * R * 4];  // one E table per warp
+    __shared__ double sP[2][R][kPStride];
+    __shared__ double sUU[32];  // U, U^-1 of the model
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int cr = threadIdx.x % G;             // CLA lane: category
+    const bool cla_ok = cr < R;
+    const int crr = cla_ok ? cr : 0;
+    const int ctiles = (v.npat + PPB - 1) / PPB;
+    const int nchunks = (v.npat + 255) / 256;
+    const int gwarp = blockIdx.x * (kThreads / 32) + warp;
+    const int nwarps = gridDim.x * (kThreads / 32);
+    int ntr = 0;
+    auto mark = [&](int code, int na) {
+        if (A.trace && blockIdx.x == 0 && threadIdx.x == 0 && ntr < A.trace_cap)
+            A.trace[ntr++] = ((unsigned long long)code << 56) | ((unsigned long long)(na & 0xffff) << 40) |
+                             (global_ns() & ((1ULL << 40) - 1));
+    };
+    for (int ci = 0; ci < A.ncmd; ci++) {
+        const BCmd cmd = A.cmds[ci];
+        mark(cmd.type == kBLevel ? kBtLevel : kBtNewton, cmd.b);
+        if (cmd.type == kBLevel) {
+            const int tpi = A.tiles_per_item;
+            const int items_per_op = (ctiles + tpi - 1) / tpi;
+            const long long nitems = (long long)cmd.b * items_per_op;
+            int cur = -1;
+            DevOp op;
+            for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+                const int j = (int)(item / items_per_op);
+                const int t0 = (int)(item % items_per_op) * tpi;
+                if (j != cur) {  // uniform across the block
+                    cur = j;
+                    op = A.ops[cmd.a + j];
+                    __syncthreads();
+                    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+                        const int mi = q / (R * 16), rem = q % (R * 16);
+                        sP[mi][rem / 16][rem % 16] =
+                            __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
+                    }
+                    __syncthreads();
+                }
+                cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, cla_ok);
+            }
+            if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtCmdDone, 0);
+            continue;
+        }
+        const int n = cmd.b;
+        const MEntry *ents = A.entries + cmd.a;
+        BSlot *slots = A.slots + cmd.a;
+        if (cmd.type == kBCoef) {
+            // work items = (entry, run of CLA-sized tiles); the entry's P blocks,
+            // U and U^-1 in shared memory
+            const int tpi = A.tiles_per_item;
+            const int items_per_entry = (ctiles + tpi - 1) / tpi;
+            const long long nitems = (long long)n * items_per_entry;
+            int loaded = -1;
+            MEntry en;
+            for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+                const int e = (int)(item / items_per_entry);
+                const int t0 = (int)(item % items_per_entry) * tpi;
+                if (e != loaded) {  // uniform across the block
+                    loaded = e;
+                    en = ents[e];
+                    __syncthreads();
+                    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+                        const int mi = q / (R * 16), rem = q % (R * 16);
+                        const int mat = mi ? en.m2 : en.m1;
+                        sP[mi][rem / 16][rem % 16] = mat >= 0 ? __ldcg(v.mats + (long long)mat * v.mat_stride + rem) : 0.0;
+                    }
+                    for (int q = threadIdx.x; q < 32; q += blockDim.x) sUU[q] = __ldg(A.eig + 4 + q);
+                    __syncthreads();
+                }
+                coef_tiles_m<R>(v, A, en, en.m1 >= 0 ? sP[0][crr] : nullptr, en.m2 >= 0 ? sP[1][crr] : nullptr, sUU,
+                                sUU + 16, e, t0, min(ctiles, t0 + tpi), crr, cla_ok);
+            }
+            if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtCmdDone, 0);
+            continue;
+        }
+        const bool newton = cmd.type == kBNewton;
+        // start: Newton states and e tables at the current lengths, everyone active
+        for (int e = gwarp; e < n; e += nwarps) {
+            const double t = __ldcg(A.lengths + ents[e].mk);
+            if (newton && lane == 0) {
+                nr_init(slots[e].st, t, A.prm.min_brlen, A.prm.max_brlen);
+                slots[e].evals = 0;
+            }
+            etab_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t, A.etab + (long long)e * 3 * R * 4);
+            if (lane == 0) A.active[e] = e;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            A.nactive[0] = n;
+            A.nactive[1] = 0;
+        }
+        if (!grid_barrier(A.gs, v.status)) return;
+        int cur = 0;
+        for (;;) {
+            const int na = *(volatile int *)(A.nactive + cur);
+            if (na == 0) break;
+            const int *act = A.active + cur * A.max_entries;
+            // (A) sweeps: a warp takes (entry, run of chunks)
+            const int cpi = A.chunks_per_item;
+            const int items_per_entry = (nchunks + cpi - 1) / cpi;
+            const long long nitems = (long long)na * items_per_entry;
+            int loaded = -1;
+            for (long long item = gwarp; item < nitems; item += nwarps) {
+                const int k = (int)(item / items_per_entry);
+                const int c0 = (int)(item % items_per_entry) * cpi;
+                const int e = __ldcg(act + k);
+                if (e != loaded) {
+                    loaded = e;
+                    __syncwarp();
+                    for (int q = lane; q < 3 * R * 4; q += 32) sE[warp][q] = __ldcg(A.etab + (long long)e * 3 * R * 4 + q);
+                    __syncwarp();
+                }
+                const int c1 = min(nchunks, c0 + cpi);
+                for (int c = c0; c < c1; c++)
+                    sweep_chunk<R>(v, A, e, sE[warp], c, A.chunk_sums + ((long long)k * nchunks + c) * 3);
+            }
+            if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtSweepDone, na);
+            if (blockIdx.x == 0 && threadIdx.x == 0) A.nactive[cur] = 0;
+            // (B) one warp per active entry
+            const int nxt = cur ^ 1;
+            for (int k = gwarp; k < na; k += nwarps) {
+                const int e = __ldcg(act + k);
+                double L, d1, d2;
+                warp_sum_chunks(A.chunk_sums + (long long)k * nchunks * 3, nchunks, L, d1, d2);
+                int fin = 1;
+                double t = 0.0;
+                if (lane == 0) {
+                    BSlot &s = slots[e];
+                    if (newton) {
+                        if (s.evals == 0) s.first_lnL = L;
+                        s.lnL = L;
+                        s.d1 = d1;
+                        s.d2 = d2;
+                        s.evals++;
+                        fin = nr_step(s.st, d1, d2, L, A.prm.precision, A.prm.min_brlen, A.prm.max_brlen);
+                        A.lengths[ents[e].mk] = s.st.v;
+                        t = s.st.v;
+                    } else {
+                        s.score = L;
+                    }
+                }
+                if (newton) {
+                    fin = __shfl_sync(0xffffffffu, fin, 0);
+                    t = __shfl_sync(0xffffffffu, t, 0);
+                    etab_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t, A.etab + (long long)e * 3 * R * 4);
+                    pmat4_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t,
+                                  const_cast<double *>(v.mats) + (long long)ents[e].mk * v.mat_stride);
+                    if (!fin && lane == 0) {
+                        const int idx = atomicAdd(A.nactive + nxt, 1);
+                        A.active[nxt * A.max_entries + idx] = e;
+                    }
+                }
+            }
+            if (!grid_barrier(A.gs, v.status)) return;
+            mark(kBtStepDone, na);
+            cur = nxt;
+        }
+        if (!grid_barrier(A.gs, v.status)) return;
+        mark(kBtCmdDone, 0);
+    }
+}
+
+}  // namespace gb

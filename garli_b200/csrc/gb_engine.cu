@@ -17,6 +17,7 @@
 
 #include "../../include/garli_b200.h"
 #include "gb_batch.cuh"
+#include "gb_batch_mixed.cuh"
 #include "gb_common.cuh"
 #include "gb_dna.cuh"
 #include "gb_graph.cuh"
@@ -104,6 +105,10 @@ struct Instance {
     int *d_active = nullptr;  // 2 x cap_bentries, then 2 counters
     size_t cap_bcmds = 0, cap_bops = 0, cap_bentries = 0, cap_bslots = 0, cap_chunk = 0, cap_active = 0;
     int batch_tiles = 0, batch_chunks = 0;  // 0: autotune on the next call
+    MEntry *d_mentries = nullptr;  // precision form: spectral coefficients per step
+    double *d_coef = nullptr, *d_etab = nullptr;
+    int *d_cscale = nullptr;
+    size_t cap_mentries = 0, cap_coef = 0, cap_etab = 0, cap_cscale = 0;
     cudaGraph_t bgraph = nullptr;
     cudaGraphExec_t bgraph_exec = nullptr;
     unsigned long long bgraph_key = 0;
@@ -118,7 +123,7 @@ static std::vector<Instance *> g_inst;
 
 // precision form: a pattern with at least this count keeps FP64 CLAs (its
 // rounding error would be multiplied by the count in the lnL sum)
-constexpr int kHeavyCount = 16;
+constexpr int kHeavyCount = 2;
 
 static Instance *get(int h) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -505,7 +510,7 @@ int gb_finalize_instance(int instance) {
                     I->d_eigen, I->d_freqs, I->d_rates, I->d_rprobs, I->d_status, I->d_block_sums,
                     I->d_result, I->d_site_lnl, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
                     I->d_cmds, I->d_pops, I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots,
-                    I->d_chunk_sums, I->d_active};
+                    I->d_chunk_sums, I->d_active, I->d_mentries, I->d_coef, I->d_etab, I->d_cscale};
     if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
     if (I->bgraph) cudaGraphDestroy(I->bgraph);
     for (void *p : ptrs)
@@ -1447,15 +1452,29 @@ static int grow_device(T **p, size_t *cap, size_t need) {
 struct BatchPlan {
     std::vector<BCmd> cmds;
     std::vector<DevOp> ops;
-    std::vector<BEntry> entries;
+    std::vector<BEntry> entries;    // plain form
+    std::vector<MEntry> mentries;   // precision form
     int max_entries = 0;
     unsigned long long key = 0;
 };
 
+static void *batch4m_func(int R) {
+    switch (R) {
+        case 1: return (void *)k_batch4m<1>;
+        case 2: return (void *)k_batch4m<2>;
+        case 3: return (void *)k_batch4m<3>;
+        case 4: return (void *)k_batch4m<4>;
+        case 5: return (void *)k_batch4m<5>;
+        case 6: return (void *)k_batch4m<6>;
+        case 7: return (void *)k_batch4m<7>;
+        default: return (void *)k_batch4m<8>;
+    }
+}
+
 // Enqueue one batched pass on the instance stream (no synchronisation).
 static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery, int tiles, int chunks,
                          bool use_graph) {
-    void *func = batch4_func(I->R, !I->mixed);
+    void *func = I->mixed ? batch4m_func(I->R) : batch4_func(I->R, true);
     int per_sm = 0;
     GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
     if (per_sm < 1) {
@@ -1464,6 +1483,28 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     }
     View v = make_view(I);
     v.rescale_every = rescaleEvery;
+    MixedArgs M;
+    M.cmds = I->d_bcmds;
+    M.ncmd = (int)P.cmds.size();
+    M.ops = I->d_bops;
+    M.entries = I->d_mentries;
+    M.slots = I->d_bslots;
+    M.prm = prm;
+    M.lengths = I->d_len;
+    M.eig = I->d_eigen;
+    M.rates = I->d_rates;
+    M.coef = I->d_coef;
+    M.cscale = I->d_cscale;
+    M.etab = I->d_etab;
+    M.chunk_sums = I->d_chunk_sums;
+    M.active = I->d_active;
+    M.nactive = I->d_active + 2 * P.max_entries;
+    M.max_entries = P.max_entries;
+    M.gs = I->d_gsync;
+    M.tiles_per_item = tiles;
+    M.chunks_per_item = chunks;
+    M.trace = use_graph ? I->d_trace : nullptr;
+    M.trace_cap = I->trace_cap;
     BatchArgs A;
     A.cmds = I->d_bcmds;
     A.ncmd = (int)P.cmds.size();
@@ -1481,7 +1522,11 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     A.gs = I->d_gsync;
     A.tiles_per_item = tiles;
     A.chunks_per_item = chunks;
-    void *args[] = {&v, &A};
+    A.trace = use_graph ? I->d_trace : nullptr;
+    A.trace_cap = I->trace_cap;
+    void *args_plain[] = {&v, &A};
+    void *args_mixed[] = {&v, &M};
+    void **args = I->mixed ? args_mixed : args_plain;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(per_sm * I->nsm);
     cfg.blockDim = dim3(kThreads);
@@ -1493,7 +1538,8 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const unsigned long long gkey = P.key ^ ((unsigned long long)tiles << 40) ^ ((unsigned long long)chunks << 48) ^
-                                    ((unsigned long long)rescaleEvery << 56);
+                                    ((unsigned long long)rescaleEvery << 56) ^
+                                    (reinterpret_cast<unsigned long long>(I->d_trace) * 0x9E3779B97F4A7C15ULL);
     if (use_graph && I->use_batch_graph) {
         if (gkey != I->bgraph_key || !I->bgraph_exec) {
             if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
@@ -1548,11 +1594,13 @@ static int autotune_batch(Instance *I, const BatchPlan &P, NrParams prm, int res
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int tiles_c[] = {1, 2, 4, 8};
+    const int tiles_plain[] = {1, 2, 4, 8}, tiles_mixed[] = {4, 8, 16, 32};
+    const int *tiles_c = I->mixed ? tiles_mixed : tiles_plain;
     const int chunks_c[] = {1, 2, 4};
     float best = 1e30f;
     int bt = 1, bc = 1, rc = GB_SUCCESS;
-    for (int t : tiles_c) {
+    for (int ti = 0; ti < 4; ti++) {
+        const int t = tiles_c[ti];
         for (int c : chunks_c) {
             for (int rep = 0; rep < 2 && rc == GB_SUCCESS; rep++) {  // first run warms up
                 cudaMemcpyAsync(I->d_len, save, len_bytes, cudaMemcpyDeviceToDevice, I->stream);
@@ -1627,7 +1675,47 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
     };
     if (rc == GB_SUCCESS)
         for (auto &lv : levels) add_level(lv);
-    for (int k = 0; k < K && rc == GB_SUCCESS; k++) {
+    for (int k = 0; k < K && rc == GB_SUCCESS && I->mixed; k++) {
+        // precision form: the step's partial is formed inside the coefficient pass
+        BCmd cc;
+        cc.type = kBCoef;
+        cc.a = (int)P.mentries.size();
+        cc.b = nC;
+        auto side = [&](int b, int &idx, int &tip) {
+            tip = b < I->ntip;
+            idx = tip ? b : b - I->ntip;
+        };
+        for (int c = 0; c < nC; c++) {
+            const gb_batch_step &s = steps[c * K + k];
+            MEntry m;
+            if (s.claOp >= 0) {
+                const gb_cla_operation &o = stepOps[s.claOp];
+                if (o.childClaIndex1 < 0 || o.childClaIndex1 >= I->ntip + I->nbuf || o.childClaIndex2 < 0 ||
+                    o.childClaIndex2 >= I->ntip + I->nbuf || o.transMatIndex1 < 0 || o.transMatIndex1 >= I->nmat ||
+                    o.transMatIndex2 < 0 || o.transMatIndex2 >= I->nmat)
+                    rc = GB_ERROR_OUT_OF_RANGE;
+                side(o.childClaIndex1, m.b1, m.t1);
+                side(o.childClaIndex2, m.b2, m.t2);
+                m.m1 = o.transMatIndex1;
+                m.m2 = o.transMatIndex2;
+            } else {
+                side(s.partialIndex, m.b1, m.t1);
+                m.m1 = -1;
+                m.b2 = -1;
+                m.t2 = 0;
+                m.m2 = -1;
+            }
+            side(s.childIndex, m.bk, m.tk);
+            m.mk = s.transMatIndex;
+            P.mentries.push_back(m);
+        }
+        P.cmds.push_back(cc);
+        BCmd nc = cc;
+        nc.type = kBNewton;
+        P.cmds.push_back(nc);
+    }
+    if (I->mixed) key = fnv(key, P.mentries.data(), sizeof(MEntry) * P.mentries.size());
+    for (int k = 0; k < K && rc == GB_SUCCESS && !I->mixed; k++) {
         std::vector<gb_cla_operation> sops;
         for (int c = 0; c < nC; c++)
             if (steps[c * K + k].claOp >= 0) {
@@ -1669,20 +1757,31 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
     key = fnv(key, &I->version, sizeof(I->version));
     P.key = key;
     const int nchunks = (I->npat + kChunk - 1) / kChunk;
+    const size_t nent = I->mixed ? P.mentries.size() : P.entries.size();
     bool realloc = false;
     {
-        const void *before[] = {I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots, I->d_chunk_sums, I->d_active};
+        const void *before[] = {I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots, I->d_chunk_sums, I->d_active,
+                                I->d_mentries, I->d_coef, I->d_cscale, I->d_etab};
+        if (I->mixed &&
+            ((rc = grow_device(&I->d_mentries, &I->cap_mentries, nent)) ||
+             (rc = grow_device(&I->d_coef, &I->cap_coef, (size_t)nC * I->R * 4 * I->npat_pad)) ||
+             (rc = grow_device(&I->d_cscale, &I->cap_cscale, (size_t)nC * I->npat_pad)) ||
+             (rc = grow_device(&I->d_etab, &I->cap_etab, (size_t)nC * 3 * I->R * 4)))) {
+            I->rank = rank_before;
+            return rc;
+        }
         if ((rc = grow_device(&I->d_bcmds, &I->cap_bcmds, P.cmds.size())) ||
             (rc = grow_device(&I->d_bops, &I->cap_bops, std::max<size_t>(1, P.ops.size()))) ||
-            (rc = grow_device(&I->d_bentries, &I->cap_bentries, P.entries.size())) ||
-            (rc = grow_device(&I->d_bslots, &I->cap_bslots, P.entries.size())) ||
+            (rc = grow_device(&I->d_bentries, &I->cap_bentries, std::max<size_t>(1, P.entries.size()))) ||
+            (rc = grow_device(&I->d_bslots, &I->cap_bslots, nent)) ||
             (rc = grow_device(&I->d_chunk_sums, &I->cap_chunk, (size_t)nC * nchunks * 3)) ||
             (rc = grow_device(&I->d_active, &I->cap_active, (size_t)2 * nC + 2))) {
             I->rank = rank_before;
             return rc;
         }
-        const void *after[] = {I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots, I->d_chunk_sums, I->d_active};
-        for (int i = 0; i < 6; i++) realloc = realloc || before[i] != after[i];
+        const void *after[] = {I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots, I->d_chunk_sums, I->d_active,
+                               I->d_mentries, I->d_coef, I->d_cscale, I->d_etab};
+        for (int i = 0; i < 10; i++) realloc = realloc || before[i] != after[i];
     }
     if (realloc) I->bgraph_key = 0;
     GB_CUDA(cudaMemcpyAsync(I->d_bcmds, P.cmds.data(), P.cmds.size() * sizeof(BCmd), cudaMemcpyHostToDevice,
@@ -1690,8 +1789,12 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
     if (!P.ops.empty())
         GB_CUDA(cudaMemcpyAsync(I->d_bops, P.ops.data(), P.ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice,
                                 I->stream));
-    GB_CUDA(cudaMemcpyAsync(I->d_bentries, P.entries.data(), P.entries.size() * sizeof(BEntry),
-                            cudaMemcpyHostToDevice, I->stream));
+    if (!P.entries.empty())
+        GB_CUDA(cudaMemcpyAsync(I->d_bentries, P.entries.data(), P.entries.size() * sizeof(BEntry),
+                                cudaMemcpyHostToDevice, I->stream));
+    if (!P.mentries.empty())
+        GB_CUDA(cudaMemcpyAsync(I->d_mentries, P.mentries.data(), P.mentries.size() * sizeof(MEntry),
+                                cudaMemcpyHostToDevice, I->stream));
     NrParams prm{precision, minLength, maxLength};
     if (I->batch_tiles == 0 || I->batch_chunks == 0) {
         if ((rc = autotune_batch(I, P, prm, rescaleEvery))) {
@@ -1703,7 +1806,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         I->rank = rank_before;
         return rc;
     }
-    std::vector<BSlot> slots(P.entries.size());
+    std::vector<BSlot> slots(nent);
     GB_CUDA(cudaMemcpyAsync(slots.data(), I->d_bslots, slots.size() * sizeof(BSlot), cudaMemcpyDeviceToHost,
                             I->stream));
     GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));

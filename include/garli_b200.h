@@ -196,7 +196,9 @@ int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, 
  * device command queue; 0: as a CUDA graph with a conditional WHILE node per branch */
 int gb_set_pass_mode(int instance, int persistent);
 /* instrumentation: phase timestamps of the persistent pass kernel, each
- * (phase code << 56) | %globaltimer ns; capacity 0 switches recording off */
+ * (phase code << 56) | %globaltimer ns, and of the batched pass kernel, each
+ * (phase code << 56) | (active candidates << 40) | low 40 bits of %globaltimer;
+ * capacity 0 switches recording off */
 int gb_set_pass_trace(int instance, int capacity);
 int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 /* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
