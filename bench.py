@@ -1,22 +1,30 @@
 """Benchmark of the B200 likelihood engine (one JSON line on rank 0).
 
-Workload (one "step"), on the 128-taxon x 100,000-site GTR+I+G4 alignment
-(synthetic, seeded; GARLI-compressed to unique patterns):
-  1. every CLA dirty and the branch lengths reset to their starting values,
-  2. a full-tree rescore (126 CLA updates + root lnL),
-  3. one all-branch Newton-Raphson pass (OptimizeAllBranches: d1/d2 per branch,
-     the CLAs each move dirties recomputed on the way).
-Metric: CLA site-updates per second (pattern x CLA update) over the whole step;
-lnL evaluations per second (full scores + edge lnL/d1/d2 evaluations) beside it.
-The headline form is the precision form (FP32 CLAs, power-of-two scalers,
-FP64 P(t)/sums/Newton); the plain FP64 form is measured in the same run.
+Headline workload (one "step" = one GA generation): 256 candidate trees, each a
+64-taxon Yule base tree after one SPR/NNI move (radius ~ U{1..8}), DNA GTR+G4,
+50,000 sites (seeded synthetic, GARLI-compressed to unique patterns).  Every
+candidate is rescored (its dirty CLAs recomputed, every other CLA shared with
+the base tree) and the three branches at its move's connector are optimised by
+GARLI's Newton-Raphson (nd->left, nd, nd->right), then scored at the optimised
+lengths.
+  * batched precision form (the headline value): all candidates in one
+    persistent kernel launch (FP32 CLAs, FP64 coefficients, sums and Newton);
+  * plain FP64 per-tree path (measured in the same run): GARLI's way, one
+    candidate after another, a host Newton loop per branch.
+Metric: CLA site-updates per second (pattern x CLA update; the per-step
+partials on the connector count as updates in both forms); lnL evaluations per
+second (edge evaluations: Newton derivative evaluations + final scores) beside it.
+The single-tree step of the 128-taxon x 100,000-site GTR+I+G4 alignment
+(full rescore + all-branch Newton pass) is reported as a secondary object.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times GARLI's CPU path (the oracle restatement, built with
-GARLI's -O3 -ffast-math flags, OpenMP over patterns on all host cores) on the
-same workload and metric.  N > 1 runs N independent replicas (one per GPU, no
-data-path collective); value = all replicas' site-updates / max-over-ranks time.
+GARLI's -O3 -ffast-math flags, OpenMP over patterns on all host cores) on a
+bounded sample of the same generation: per candidate the CLAs GARLI would
+recompute after the move, the same three Newton optimisations and the final
+score.  N > 1 runs N independent replicas (one per GPU, no data-path
+collective); value = all replicas' site-updates / max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -34,21 +42,29 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "CLA site-updates/s (128x100k GTR+I+G4: full rescore + all-branch Newton pass)"
+METRIC = ("CLA site-updates/s (GA generation: 256 SPR/NNI candidates of a 64-taxon tree, 50k sites, GTR+G4; "
+          "rescore + 3-branch Newton each), batched precision form")
 UNIT = "site-updates/s"
+SINGLE_METRIC = "CLA site-updates/s (128x100k GTR+I+G4: full rescore + all-branch Newton pass)"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ntax", type=int, default=128)
-    ap.add_argument("--nsites", type=int, default=100_000)
+    ap.add_argument("--ncand", type=int, default=256)
+    ap.add_argument("--batch-ntax", type=int, default=64)
+    ap.add_argument("--batch-nsites", type=int, default=50_000)
+    ap.add_argument("--ntax", type=int, default=128, help="single-tree workload")
+    ap.add_argument("--nsites", type=int, default=100_000, help="single-tree workload")
     ap.add_argument("--precision", type=float, default=0.01, help="Newton optPrecision")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-sites", type=int, default=20_000)
+    ap.add_argument("--no-single", action="store_true", help="skip the single-tree secondary measurement")
+    ap.add_argument("--cpu-sample-cands", type=int, default=24, help="candidates in the CPU baseline sample")
+    ap.add_argument("--cpu-repeats", type=int, default=16, help="timed repeats per sampled candidate")
+    ap.add_argument("--ref-cands-per-step", type=int, default=2, help="candidates per --impl reference step")
     return ap.parse_args()
 
 
@@ -117,13 +133,19 @@ def peaks():
 
 
 def profiled_traffic():
-    """Per-launch DRAM bytes of the CLA kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "cla_kernel_traffic.json")
+    """Per-launch DRAM bytes of the batched pass kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "batch_kernel_traffic.json")
     try:
         with open(path) as f:
             return json.load(f)
     except Exception:
         return None
+
+
+def batch_workload(args, seed):
+    from garli_b200 import synth
+
+    return synth.batch_workload(seed=seed, ntax=args.batch_ntax, nsites=args.batch_nsites, ncand=args.ncand)
 
 
 def make_workload(args, seed):
@@ -201,86 +223,214 @@ def run_form(w, args, mixed, device, steps, warmup, timing_pass=True):
             "tree": tree}
 
 
-def e2e_run(w, args, device, steps):
-    """The same step through the C ABI from host buffers: tips, weights and model are
-    uploaded every step and the site log-likelihoods and branch lengths read back."""
+def run_batch(bw, args, device, mixed, sequential, steps, warmup, clocks=None):
+    """Time `steps` generations (device-timed on the instance stream)."""
     import torch
 
     from garli_b200 import engine
 
-    pd = w.data
-    inst, tree = engine.tree_engine(pd, w.child3, w.dlen, w.model, device=device, mixed=True)
-    tips = [np.ascontiguousarray(pd.tips[t]) for t in range(pd.ntax)]
-    bi = sum(t.nbytes for t in tips) + pd.counts.nbytes + pd.const_states.nbytes + w.dlen.nbytes
-    bo = 8 * pd.npat + w.dlen.nbytes
-    one_step(tree, w.dlen, args.precision)
+    w, c3s, dls, conn = bw
+    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), device=device, mixed=mixed)
+    stream = torch.cuda.ExternalStream(inst.stream_ptr(), device=f"cuda:{device}")
+    out = lens = None
+    for _ in range(warmup):  # the first call computes the base tree's CLAs and autotunes
+        out, lens = pop.score(c3s, dls, conn, args.precision, sequential=sequential)
+    torch.cuda.synchronize(device)
+    l0 = inst.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    updates = edges = 0
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        e0.record(stream)
+        for _ in range(steps):
+            out, lens = pop.score(c3s, dls, conn, args.precision, sequential=sequential)
+            cnt = pop.counters()
+            updates += cnt["pattern_updates"]
+            edges += cnt["edge_evals"]
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1)
+    res = {"ms": ms, "updates": updates, "edges": edges, "launches": inst.launch_count() - l0, "out": out,
+           "lens": lens, "counters": pop.counters(), "tuning": pop.tuning(), "inst": inst, "pop": pop}
+    return res
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def batch_kernel_roofline(r, args, peak, peak_kind):
+    """Achieved bandwidth of k_batch4m: algorithmic bytes of one launch over its
+    CUDA-event time on the instance stream (a few extra timed passes)."""
+    import torch
+
+    w_c3s = r["bw"]
+    pop, inst = r["pop"], r["inst"]
+    _, c3s, dls, conn = w_c3s
+    inst.set_kernel_timing(True)
+    t0 = pop.batch_timing()
+    n = 5
+    for _ in range(n):
+        pop.score(c3s, dls, conn, args.precision)
+    t1 = pop.batch_timing()
+    inst.set_kernel_timing(False)
+    torch.cuda.synchronize()
+    ms = (t1["ms"] - t0["ms"]) / max(1, t1["launches"] - t0["launches"])
+    alg = pop.counters()["alg_bytes"]
+    achieved = alg / (ms / 1e3) / 1e9
+    traffic = profiled_traffic()
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic.get("bytes_per_launch") if traffic else None,
+            "kernel": "k_batch4m<4> (batched pass, one launch per generation)",
+            "peak_kind": f"{peak_kind} hbm_gbs (burst copy)", "kernel_ms_per_launch": ms,
+            "algorithmic_bytes_per_launch": alg,
+            "traffic_note": traffic.get("note") if traffic else "no ncu capture committed"}
+
+
+def e2e_batch(bw, args, device, steps):
+    """The generation through the public call with host buffers: candidate
+    topologies, lengths and connectors go in from pinned host memory, per-candidate
+    lnL / improvement / evaluations and the optimised lengths come back."""
+    import torch
+
+    from garli_b200 import engine
+
+    w, c3s, dls, conn = bw
+    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), device=device, mixed=True)
+    pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in (c3s, dls, conn)]
+    pop.score(*pin, args.precision)
+    torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     updates = 0
+    out = lens = None
     for _ in range(steps):
-        inst.set_data(pd)
-        tree.set_model(w.model)
-        lnl, d = one_step(tree, w.dlen, args.precision)
-        updates += d["pattern_updates"]
-        inst.site_lnl()
-        tree.branch_lengths()
+        out, lens = pop.score(*pin, args.precision)
+        updates += pop.counters()["pattern_updates"]
     torch.cuda.synchronize(device)
     dt = time.perf_counter() - t0
-    tree.close()
+    bi = sum(a.nbytes for a in pin)
+    bo = out.nbytes + lens.nbytes
+    pop.close()
     inst.close()
     return updates / dt, bi, bo
 
 
-def cpu_baseline(args, threads=None):
-    """GARLI's CPU path (oracle restatement, GARLI's gcc flags) on a bounded sample:
-    the same tree and model, the first ``cpu_sample_sites`` sites."""
+def single_tree(args, device, rank):
+    """Secondary: the 128x100k single-tree step, precision and plain forms."""
+    w = make_workload(args, seed=1 + rank)
+    plain = run_form(w, args, mixed=False, device=device, steps=2, warmup=1)
+    mixed = run_form(w, args, mixed=True, device=device, steps=4, warmup=2)
+    kt = mixed["kt"]
+    v = mixed["tot"]["pattern_updates"] / (mixed["ms"] / 1000.0)
+    pv = plain["tot"]["pattern_updates"] / (plain["ms"] / 1000.0)
+    res = {"metric": SINGLE_METRIC, "workload": w.name, "npat": w.data.npat, "value": v, "unit": UNIT,
+           "ms_per_step": mixed["ms"] / 4, "phases": mixed["phases"],
+           "lnl_evals_per_s": (mixed["tot"]["scores"] + mixed["tot"]["edge_evals"]) / (mixed["ms"] / 1000.0),
+           "plain_fp64": {"value": pv, "ms_per_step": plain["ms"] / 2, "phases": plain["phases"]},
+           "mixed_over_plain": v / pv, "abs_dlnl_mixed_vs_plain": abs(mixed["lnl"] - plain["lnl"]),
+           "cla_kernel_gbs": (kt["cla_bytes"] / (kt["cla_ms"] / 1000.0) / 1e9) if kt and kt["cla_ms"] > 0 else None}
+    for f in (plain, mixed):
+        f["tree"].close()
+        f["inst"].close()
+    return res
+
+
+def _oracle_candidate(w, c3, dl, X, prec, orc, repeats=1):
+    """GARLI's CPU path for one candidate: the tree is built and scored (the
+    parent's CLAs), the move's branches are touched so the CLAs GARLI would
+    recompute are dirty (SweepDirtynessOverTree), then -- timed -- the rescore,
+    the three Newton optimisations and the final score; ``repeats`` times from
+    the same starting lengths.  Returns (seconds, CLA ops)."""
+    ot = orc.OracleTree(w.data, c3, dl, w.model, fast=True)
+    ot.score(0)
+    order = [int(c3[X][0]), int(X), int(c3[X][2])]
+    tt = 0.0
+    ops = 0
+    for _ in range(repeats):
+        for nd in order:
+            ot.set_branch_length(nd, float(dl[nd]))
+        c0 = ot.counts()["cla"]
+        t0 = time.perf_counter()
+        ot.score(0)
+        for nd in order:
+            ot.optimize_branch(nd, prec)
+        ot.make_all_dirty()
+        ot.score(int(X))
+        tt += time.perf_counter() - t0
+        ops += ot.counts()["cla"] - c0
+    ot.close()
+    return tt, ops
+
+
+def cpu_baseline(args, bw):
+    """GARLI's CPU path (oracle restatement, GARLI's gcc flags, OpenMP over
+    patterns on all cores) on a bounded sample of the generation."""
     from oracle import oracle as orc
 
-    wsamp = make_workload(argparse.Namespace(ntax=args.ntax, nsites=args.cpu_sample_sites), seed=1)
-    cores = threads or os.cpu_count() or 1
+    w, c3s, dls, conn = bw
+    cores = os.cpu_count() or 1
     orc.set_threads(cores, fast=True)
-    ot = orc.OracleTree(wsamp.data, wsamp.child3, wsamp.dlen, wsamp.model, fast=True)
-    t0 = time.perf_counter()
-    c0 = ot.counts()["cla"]
-    ot.make_all_dirty()
-    ot.score(0)
-    ot.optimize_all_branches(args.precision)
-    dt = time.perf_counter() - t0
-    ops = ot.counts()["cla"] - c0
-    ot.close()
-    return {"value": ops * wsamp.data.npat / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{args.ntax} taxa x {args.cpu_sample_sites} sites ({wsamp.data.npat} patterns), "
-                      f"1 step = rescore + all-branch Newton pass, {dt:.1f} s"}
+    k = min(args.cpu_sample_cands, len(conn))
+    tt = 0.0
+    ops = 0
+    reps = max(1, args.cpu_repeats)
+    for i in range(k):
+        dt, o = _oracle_candidate(w, c3s[i], dls[i], int(conn[i]), args.precision, orc, repeats=reps)
+        tt += dt
+        ops += o
+    return {"value": ops * w.data.npat / tt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{k} of {len(conn)} candidates x {reps} repeats ({w.data.npat} patterns): dirty-CLA "
+                      f"rescore + 3-branch Newton + final score each, {tt:.1f} s timed"}
 
 
 def reference_arm(args, ws, rank):
     if rank != 0:
         return
-    steps = max(1, args.steps)
     from oracle import oracle as orc
 
+    bw = batch_workload(args, seed=4)
+    w, c3s, dls, conn = bw
     cores = os.cpu_count() or 1
-    wsamp = make_workload(args, seed=1)
     orc.set_threads(cores, fast=True)
-    ot = orc.OracleTree(wsamp.data, wsamp.child3, wsamp.dlen, wsamp.model, fast=True)
-    for _ in range(min(args.warmup, 1)):
-        ot.make_all_dirty(); ot.score(0)
-    t0 = time.perf_counter()
-    c0 = ot.counts()["cla"]
-    for _ in range(steps):
-        for nd in range(1, len(wsamp.dlen)):
-            ot.set_branch_length(nd, float(wsamp.dlen[nd]))
-        ot.make_all_dirty()
-        ot.score(0)
-        ot.optimize_all_branches(args.precision)
-    dt = time.perf_counter() - t0
-    v = (ot.counts()["cla"] - c0) * wsamp.data.npat / dt
+    per = max(1, args.ref_cands_per_step)
+    nxt = 0
+
+    def step():
+        nonlocal nxt
+        t = 0.0
+        o = 0
+        for _ in range(per):
+            i = nxt % len(conn)
+            nxt += 1
+            dt, ops = _oracle_candidate(w, c3s[i], dls[i], int(conn[i]), args.precision, orc)
+            t += dt
+            o += ops
+        return t, o
+
+    for _ in range(args.warmup):
+        step()
+    tt = 0.0
+    ops = 0
+    for _ in range(max(1, args.steps)):
+        dt, o = step()
+        tt += dt
+        ops += o
+    v = ops * w.data.npat / tt
+    steps = max(1, args.steps)
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wsamp.name, "ntax": args.ntax, "nsites": args.nsites, "npat": wsamp.data.npat,
-                       "model": "GTR+I+G4", "form": "GARLI CPU path, FP64", "parallelism": "openmp-patterns"},
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1000 * tt / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "ntax": args.batch_ntax, "nsites": args.batch_nsites,
+                       "npat": w.data.npat, "candidates": len(conn), "model": "GTR+G4",
+                       "form": "GARLI CPU path, FP64, one candidate at a time", "parallelism": "openmp-patterns"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{steps} step(s) of the full {args.ntax}x{args.nsites} workload"},
+                             "sample": f"{per} candidate(s) per step (cycling through the generation): dirty-CLA "
+                                       "rescore + 3-branch Newton + final score each"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -303,73 +453,79 @@ def main():
         pg = dist
     device = local if ws > 1 else 0
     torch.cuda.set_device(device)
-    w = make_workload(args, seed=1 + rank)
     peak, peak_kind = peaks()
+    bw = batch_workload(args, seed=4 + rank)
+    w, c3s, dls, conn = bw
 
-    # plain FP64 form (same workload, fewer steps)
-    plain = run_form(w, args, mixed=False, device=device, steps=max(1, args.steps // 2), warmup=1)
-    # precision form: the headline
+    # plain FP64 per-tree path (GARLI's way), same generation
+    plain = run_batch(bw, args, device, mixed=False, sequential=True, steps=max(1, args.steps // 20), warmup=1)
+    # headline: batched precision form
     if pg:
         pg.barrier()
-    with ClockSampler(device) as clk:
-        mixed = run_form(w, args, mixed=True, device=device, steps=args.steps, warmup=args.warmup)
+    torch.cuda.synchronize(device)
+    clk = ClockSampler(device)
+    mixed = run_batch(bw, args, device, mixed=True, sequential=False, steps=args.steps, warmup=args.warmup,
+                      clocks=clk)
+    torch.cuda.synchronize(device)
+    if pg:
+        pg.barrier()
     ms = mixed["ms"]
+    updates = float(mixed["updates"])
+    edges = float(mixed["edges"])
     if pg:
         t = torch.tensor([ms], dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
-        u = torch.tensor([float(mixed["tot"]["pattern_updates"])], dtype=torch.float64)
+        u = torch.tensor([updates, edges], dtype=torch.float64)
         pg.all_reduce(u)
-        updates_all = float(u.item())
-    else:
-        updates_all = float(mixed["tot"]["pattern_updates"])
-    value = updates_all / (ms / 1000.0)
-    evals = mixed["tot"]["scores"] + mixed["tot"]["edge_evals"]
-    plain_v = plain["tot"]["pattern_updates"] / (plain["ms"] / 1000.0)
-    kt = mixed["kt"]
-    achieved = kt["cla_bytes"] / (kt["cla_ms"] / 1000.0) / 1e9 if kt and kt["cla_ms"] > 0 else None
-    traffic = profiled_traffic()
-    e2e_v, bi, bo = e2e_run(w, args, device, max(1, args.steps // 2))
+        updates, edges = float(u[0]), float(u[1])
+    value = updates / (ms / 1000.0)
+    plain_v = plain["updates"] / (plain["ms"] / 1000.0)
+    mixed["bw"] = bw
+    roof = batch_kernel_roofline(mixed, args, peak, peak_kind)
+    d0 = float(np.abs(mixed["out"][:, 0] - plain["out"][:, 0]).max())
+    d1 = float(np.abs(mixed["out"][:, 1] - plain["out"][:, 1]).max())
+    dlen = float(np.max(np.abs(mixed["lens"] - plain["lens"]) / np.maximum(plain["lens"], 1e-8)))
+    tuning = mixed["tuning"]
+    cnt = mixed["counters"]
+    for f in (plain, mixed):
+        f["pop"].close()
+        f["inst"].close()
+    e2e_v, bi, bo = e2e_batch(bw, args, device, max(3, args.steps // 4))
     if pg:
         t = torch.tensor([e2e_v], dtype=torch.float64)
         pg.all_reduce(t)
         e2e_v = float(t.item())
-    # precision form vs plain FP64 on the same tree (the rescore at the starting lengths);
-    # the oracle itself is checked in tests/
-    dl = abs(mixed["lnl"] - plain["lnl"])
+    single = None if args.no_single else single_tree(args, device, rank)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args)
+        cpu = cpu_baseline(args, bw)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32-cla/f64-sums", "data": "synthetic (seeded)",
-            "config": {"workload": w.name, "ntax": args.ntax, "nsites": args.nsites, "npat": w.data.npat,
-                       "model": "GTR+I+G4", "form": "precision (FP32 CLAs, pow2 scalers)",
-                       "step": "reset + full rescore + all-branch Newton pass",
-                       "l2": "working set > L2 (378 CLAs x 4.3 MB)", "parallelism": f"replicas{ws}"},
-            "lnl_evals_per_s": evals * ws / (ms / 1000.0),
-            "plain_fp64": {"value": plain_v, "unit": UNIT, "ms_per_step": plain["ms"] / max(1, args.steps // 2),
-                           "lnl": plain["lnl"], "phases": plain["phases"]},
-            "phases": mixed["phases"],
-            "mixed_over_plain": value / ws / plain_v,
-            "abs_dlnl_mixed_vs_plain_same_tree": dl,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-cla/f64-coef-sums-newton",
+            "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "ntax": args.batch_ntax, "nsites": args.batch_nsites,
+                       "npat": w.data.npat, "candidates": len(conn), "moves": "SPR radius U{1..8} (1 = NNI)",
+                       "model": "GTR+G4", "form": "batched precision (FP32 CLAs, pow2 scalers, FP64 Newton)",
+                       "step": "one generation: dirty-CLA rescore + 3-branch Newton + final score per candidate",
+                       "cla_updates_per_step": cnt["cla_ops"], "l2": "working set > L2 (coefficients 1.2 GB)",
+                       "tuning": tuning, "parallelism": f"replicas{ws}"},
+            "lnl_evals_per_s": edges / (ms / 1000.0),
+            "plain_per_tree": {"value": plain_v, "unit": UNIT, "form": "plain FP64, per candidate, host Newton loop",
+                               "ms_per_step": plain["ms"] / max(1, args.steps // 20),
+                               "lnl_evals_per_s": plain["edges"] / (plain["ms"] / 1000.0)},
+            "mixed_over_plain": (value / ws) / plain_v,
+            "max_abs_dlnl_vs_plain": {"rescore": d0, "optimised": d1, "max_rel_dlen": dlen},
             "gpu_launches": mixed["launches"],
             "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None,
-                         "traffic": traffic.get("bytes_per_launch") if traffic else None,
-                         "kernel": "k_cla4<float,4> (CLA update)", "peak_kind": f"{peak_kind} hbm_gbs",
-                         "cla_kernel_ms_per_step": kt["cla_ms"] if kt else None,
-                         "edge_kernel_ms_per_step": kt["edge_ms"] if kt else None},
+            "roofline": roof,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "single_tree": single,
         }
         print(json.dumps(line), flush=True)
-    for f in (plain, mixed):
-        f["tree"].close()
-        f["inst"].close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

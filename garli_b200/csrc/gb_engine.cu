@@ -113,6 +113,8 @@ struct Instance {
     cudaGraphExec_t bgraph_exec = nullptr;
     unsigned long long bgraph_key = 0;
     int use_batch_graph = 1;
+    double batch_ms = 0.0;  // CUDA-event time of the timed batched launches
+    long long batch_timed = 0;
 
     long long mat_stride() const { return 3LL * R * S * S; }
     long long eig_stride() const { return (long long)S + 2LL * S * S; }
@@ -1802,15 +1804,30 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
             return rc;
         }
     }
+    cudaEvent_t te0 = nullptr, te1 = nullptr;
+    if (I->timing) {
+        cudaEventCreate(&te0);
+        cudaEventCreate(&te1);
+        cudaEventRecord(te0, I->stream);
+    }
     if ((rc = enqueue_batch(I, P, prm, rescaleEvery, I->batch_tiles, I->batch_chunks, true))) {
         I->rank = rank_before;
         return rc;
     }
+    if (te1) cudaEventRecord(te1, I->stream);
     std::vector<BSlot> slots(nent);
     GB_CUDA(cudaMemcpyAsync(slots.data(), I->d_bslots, slots.size() * sizeof(BSlot), cudaMemcpyDeviceToHost,
                             I->stream));
     GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
+    if (te1) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, te0, te1);
+        I->batch_ms += ms;
+        I->batch_timed++;
+        cudaEventDestroy(te0);
+        cudaEventDestroy(te1);
+    }
     for (int c = 0; c < nC; c++) {
         double imp = 0.0;
         long long ev = 0;
@@ -1845,6 +1862,14 @@ int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem) {
     I->batch_tiles = tilesPerItem;
     I->batch_chunks = chunksPerItem;
     I->bgraph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_get_batch_timing(int instance, double *out2) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    out2[0] = I->batch_ms;
+    out2[1] = (double)I->batch_timed;
     return GB_SUCCESS;
 }
 

@@ -138,7 +138,8 @@ struct Pop {
     std::unordered_map<uint64_t, int> mat_of;  // length bits -> matrix slot
     int base_mats = 0, next_mat = 0;
     std::vector<double> mat_len;
-    long long c_ops = 0, c_updates = 0, c_evals = 0, c_base_ops = 0;
+    long long c_ops = 0, c_updates = 0, c_evals = 0, c_base_ops = 0, c_edges = 0;
+    double c_bytes = 0.0;
     int npat = 0;
 };
 
@@ -327,6 +328,24 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
     return GB_SUCCESS;
 }
 
+// Algorithmic device-memory bytes of one batched pass of the precision form
+// per pattern (R = 4 categories, FP32 CLAs): see gbp_get_counters.
+double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps) {
+    auto is_tip = [&](int b) { return b < p.ntip; };
+    double per = 0.0;
+    for (const gb_cla_operation &o : P.ops) {
+        const int t = (is_tip(o.childClaIndex1) ? 1 : 0) + (is_tip(o.childClaIndex2) ? 1 : 0);
+        per += t == 0 ? 204.0 : t == 1 ? 137.0 : 70.0;
+    }
+    for (int i = 0; i < 3 * nC; i++) {
+        const gb_cla_operation &o = P.step_ops[i];
+        per += 132.0;
+        for (int b : {o.childClaIndex1, o.childClaIndex2, P.steps[i].childIndex}) per += is_tip(b) ? 1.0 : 68.0;
+    }
+    per += 140.0 * (double)sweeps;
+    return per * (double)p.npat;
+}
+
 int upload_mats(Pop &p) {
     int rc = gb_set_branch_lengths(p.inst, p.mat_len.data(), p.next_mat);
     if (rc) return rc;
@@ -451,6 +470,8 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
             p->c_evals = 0;
             rc = run_sequential(*p, P, candidateCount, precision, out, lengthsOut);
             p->c_updates = p->c_ops * p->npat;
+            p->c_edges = p->c_evals + candidateCount;
+            p->c_bytes = plan_bytes(*p, P, candidateCount, p->c_edges);
         } else {
             rc = gb_batch_newton(p->inst, P.ops.data(), (int)P.ops.size(), P.step_ops.data(),
                                  (int)P.step_ops.size(), P.steps.data(), candidateCount, 3, p->rescaleEvery,
@@ -463,6 +484,8 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
                 p->c_updates = p->c_ops * p->npat;
                 p->c_evals = 0;
                 for (int c = 0; c < candidateCount; c++) p->c_evals += (long long)out[4 * c + 3];
+                p->c_edges = p->c_evals + candidateCount;
+                p->c_bytes = plan_bytes(*p, P, candidateCount, p->c_edges);
             }
         }
         if (rc == GB_ERROR_RESCALE_RETRY) {
@@ -476,13 +499,15 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
     }
 }
 
-int gbp_get_counters(int pop, long long *out4) {
+int gbp_get_counters(int pop, long long *out6) {
     Pop *p = get(pop);
     if (!p) return GB_ERROR_UNINITIALIZED_INSTANCE;
-    out4[0] = p->c_ops;
-    out4[1] = p->c_updates;
-    out4[2] = p->c_evals;
-    out4[3] = p->c_base_ops;
+    out6[0] = p->c_ops;
+    out6[1] = p->c_updates;
+    out6[2] = p->c_evals;
+    out6[3] = p->c_base_ops;
+    out6[4] = p->c_edges;
+    out6[5] = (long long)p->c_bytes;
     return GB_SUCCESS;
 }
 

@@ -108,6 +108,7 @@ SIGNATURES = {
                                   C.c_int, C.c_double, C.c_double, C.c_double, _D]),
     "gb_set_batch_tuning": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "gb_get_batch_tuning": (C.c_int, [C.c_int, _I]),
+    "gb_get_batch_timing": (C.c_int, [C.c_int, _D]),
     "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),
     "gbp_destroy": (C.c_int, [C.c_int]),
     "gbp_invalidate": (C.c_int, [C.c_int]),
@@ -478,10 +479,15 @@ class Population:
         return out, lens
 
     def counters(self) -> dict:
-        out = np.zeros(4, dtype=np.int64)
+        out = np.zeros(6, dtype=np.int64)
         _chk(lib().gbp_get_counters(self.h, out.ctypes.data_as(_LL)), "gbp_get_counters")
-        return {"cla_ops": int(out[0]), "pattern_updates": int(out[1]), "edge_evals": int(out[2]),
-                "base_cla_ops": int(out[3])}
+        return {"cla_ops": int(out[0]), "pattern_updates": int(out[1]), "deriv_evals": int(out[2]),
+                "base_cla_ops": int(out[3]), "edge_evals": int(out[4]), "alg_bytes": int(out[5])}
+
+    def batch_timing(self) -> dict:
+        out = np.zeros(2)
+        _chk(lib().gb_get_batch_timing(self.inst.h, _p(out, C.c_double)), "gb_get_batch_timing")
+        return {"ms": float(out[0]), "launches": int(out[1])}
 
     def tuning(self) -> dict:
         out = np.zeros(3, dtype=np.int32)

@@ -234,6 +234,9 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
 int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem);
 /* out[0..2] = tiles per item, chunks per item, 1 if the pass replays a CUDA graph */
 int gb_get_batch_tuning(int instance, int *out3);
+/* instrumentation (while gb_set_kernel_timing is on): out[0] = CUDA-event ms of
+ * the batched pass launches on the instance stream, out[1] = launches timed */
+int gb_get_batch_timing(int instance, double *out2);
 
 /* ---- population layer: a GA generation's candidates on one instance ----
  * A C++ restatement of how GARLI scores the candidates of a generation: each
@@ -259,9 +262,13 @@ int gbp_invalidate(int pop);
 int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const double *dlens,
                          const int *connectors, double precision, int sequential, double *out,
                          double *lengthsOut);
-/* last call: [0] CLA updates, [1] pattern-updates, [2] derivative evaluations;
- * [3] base-tree CLA updates since creation */
-int gbp_get_counters(int pop, long long *out4);
+/* last call: [0] CLA updates (the per-step partials included), [1] pattern-updates,
+ * [2] derivative evaluations, [4] edge evaluations (derivative evaluations + the
+ * final scores), [5] algorithmic device-memory bytes of the precision form's
+ * batched pass (FP32 CLAs: 204 / 137 / 70 B per int-int / int-tip / tip-tip
+ * pattern-update, 132 B written + 68 B per CLA side read per coefficient
+ * pattern, 140 B per edge-evaluation pattern); [3] base-tree CLA updates since creation */
+int gbp_get_counters(int pop, long long *out6);
 
 /* ---- edge evaluation without device allocation ----
  * No counterpart in the reference: GARLI's beagle build lets beagle allocate.
