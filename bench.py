@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--precision", type=float, default=0.01, help="Newton optPrecision")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single", action="store_true", help="skip the single-tree secondary measurement")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="profiling: only the batched form (no per-tree comparison, no e2e pass)")
     ap.add_argument("--cpu-sample-cands", type=int, default=24, help="candidates in the CPU baseline sample")
     ap.add_argument("--cpu-repeats", type=int, default=16, help="timed repeats per sampled candidate")
     ap.add_argument("--ref-cands-per-step", type=int, default=2, help="candidates per --impl reference step")
@@ -340,6 +342,47 @@ def single_tree(args, device, rank):
     return res
 
 
+def nstate_forms(kind, device, reps=3):
+    """Secondary: full-tree rescore of the 20-state (64 taxa x 20,000 sites, +G4)
+    or 61-state (32 taxa x 5,000 codons) alignment in the precision form with the
+    tensor-core CLA update, the same form on CUDA cores, and the plain FP64 form;
+    CLA site-updates/s (device-timed) and each form's lnL against plain FP64."""
+    import torch
+
+    from garli_b200 import engine, synth
+
+    w = synth.aa() if kind == "aa" else synth.codon()
+    out = {"workload": w.name, "npat": w.data.npat, "states": w.data.nstates, "categories": w.model.ncat}
+    ref = None
+    for name, mixed, tc in (("plain_fp64", False, False), ("precision_tensor_cores", True, True),
+                            ("precision_cuda_cores", True, False)):
+        inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model, device=device, mixed=mixed)
+        if mixed:
+            inst.set_tensor_cores(tc)
+        stream = torch.cuda.ExternalStream(inst.stream_ptr(), device=f"cuda:{device}")
+        tree.make_all_dirty()
+        lnl = tree.score(0)
+        c0 = tree.counters()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        for _ in range(reps):
+            tree.make_all_dirty()
+            tree.score(0)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        upd = tree.counters()["pattern_updates"] - c0["pattern_updates"]
+        if ref is None:
+            ref = lnl
+        out[name] = {"site_updates_per_s": upd / (ms / 1000.0), "ms_per_rescore": ms / reps, "lnl": lnl,
+                     "dlnl_vs_plain": lnl - ref}
+        tree.close()
+        inst.close()
+    return out
+
+
 def _oracle_candidate(w, c3, dl, X, prec, orc, repeats=1):
     """GARLI's CPU path for one candidate: the tree is built and scored (the
     parent's CLAs), the move's branches are touched so the CLAs GARLI would
@@ -457,6 +500,18 @@ def main():
     bw = batch_workload(args, seed=4 + rank)
     w, c3s, dls, conn = bw
 
+    if args.batch_only:
+        r = run_batch(bw, args, device, mixed=True, sequential=False, steps=args.steps, warmup=args.warmup)
+        if rank == 0:
+            print(json.dumps({"batch_only": True, "value": r["updates"] / (r["ms"] / 1000.0), "unit": UNIT,
+                              "ms_per_step": r["ms"] / args.steps, "npat": w.data.npat,
+                              "alg_bytes_per_launch": r["counters"]["alg_bytes"], "tuning": r["tuning"]}))
+        r["pop"].close()
+        r["inst"].close()
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     # plain FP64 per-tree path (GARLI's way), same generation
     plain = run_batch(bw, args, device, mixed=False, sequential=True, steps=max(1, args.steps // 20), warmup=1)
     # headline: batched precision form
@@ -497,6 +552,8 @@ def main():
         pg.all_reduce(t)
         e2e_v = float(t.item())
     single = None if args.no_single else single_tree(args, device, rank)
+    nstate = None if args.no_single else {"aa_20_states": nstate_forms("aa", device),
+                                          "codon_61_states": nstate_forms("codon", device)}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, bw)
@@ -524,6 +581,7 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "single_tree": single,
+            "nstate": nstate,
         }
         print(json.dumps(line), flush=True)
     if pg:

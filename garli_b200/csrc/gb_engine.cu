@@ -25,6 +25,7 @@
 #include "gb_nstate.cuh"
 #include "gb_persist.cuh"
 #include "gb_pmat.cuh"
+#include "gb_tc.cuh"
 
 namespace gb {
 
@@ -113,6 +114,8 @@ struct Instance {
     cudaGraphExec_t bgraph_exec = nullptr;
     unsigned long long bgraph_key = 0;
     int use_batch_graph = 1;
+    int use_tc = 1;  // precision form, 20 / 61 states: CLA updates on the tensor cores
+    double tc_corr = kTcCorrUlps;  // mean truncation loss of one UMMA result, in ulps
     double batch_ms = 0.0;  // CUDA-event time of the timed batched launches
     long long batch_timed = 0;
 
@@ -245,8 +248,39 @@ static int ns_edge_tile(const Instance *I, size_t *smem) {
     return tp;
 }
 
+// tensor-core CLA update (gb_tc.cuh): supported shapes and launch parameters
+static bool tc_supported(const Instance *I) {
+    return I->mixed && I->use_tc && ((I->S == 20 && I->R <= 8) || (I->S == 61 && I->R <= 2));
+}
+template <int S, int R>
+static size_t tc_smem_bytes() {
+    // at most 512 / COLS CTAs may share an SM's TMEM: shared memory is sized so
+    // that no more fit (an allocation would otherwise wait for a finishing CTA)
+    const int maxc = 512 / TcSmem<S, R>::COLS;
+    const size_t floor_b = 233472 / (maxc + 1) + 1024;
+    return std::min<size_t>(232448, std::max<size_t>(TcSmem<S, R>::BYTES, floor_b));
+}
+static void *tc_func(int S, int R, size_t *smem) {
+#define GB_TC(s, r)                       \
+    if (S == s && R == r) {               \
+        *smem = tc_smem_bytes<s, r>();    \
+        return (void *)k_cla_tc<s, r>;    \
+    }
+    GB_TC(20, 1) GB_TC(20, 2) GB_TC(20, 3) GB_TC(20, 4) GB_TC(20, 5) GB_TC(20, 6) GB_TC(20, 7) GB_TC(20, 8)
+    GB_TC(61, 1) GB_TC(61, 2)
+#undef GB_TC
+    *smem = 0;
+    return nullptr;
+}
+
 static int set_smem_attrs() {
     const int big = 200 * 1024;
+    for (int S : {20, 61})
+        for (int R = 1; R <= 8; R++) {
+            size_t sm = 0;
+            void *f = tc_func(S, R, &sm);
+            if (f) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        }
     GB_CUDA(cudaFuncSetAttribute(k_cla_ns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_cla_ns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -295,9 +329,22 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
         } else {
             size_t smem;
             const int tp = ns_cla_tile(I, &smem);
-            dim3 grid((I->npat + tp - 1) / tp, L.n);
-            if (I->mixed) k_cla_ns<false><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
-            else k_cla_ns<true><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
+            // precision form on the tensor cores: CUDA cores keep only the FP64 segment
+            const bool tc = tc_supported(I);
+            const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
+            if (ns_pat > 0) {
+                dim3 grid((ns_pat + tp - 1) / tp, L.n);
+                if (I->mixed) k_cla_ns<false><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
+                else k_cla_ns<true><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
+            }
+            const int first = I->kpad / kTcM, nt = I->npat_pad / kTcM - first;
+            if (tc && nt > 0) {
+                size_t tsm = 0;
+                void *f = tc_func(I->S, I->R, &tsm);
+                double corr = I->tc_corr;
+                void *args[] = {&v, &L, (void *)&first, &corr};
+                GB_CUDA(cudaLaunchKernel(f, dim3(nt, L.n), dim3(kTcM), args, tsm, I->stream));
+            }
         }
         int rc = check_launch(I);
         if (rc) return rc;
@@ -1046,11 +1093,12 @@ static void *edge4_deriv_func(int R, bool garli) {
 struct GraphBuilder {
     cudaGraph_t g;
     int nodes = 0;
+    dim3 block = dim3(kThreads);  // block size of the next node
     int add(cudaGraph_t graph, cudaGraphNode_t *prev, void *func, dim3 grid, size_t smem, void **args) {
         cudaKernelNodeParams kp = {};
         kp.func = func;
         kp.gridDim = grid;
-        kp.blockDim = dim3(kThreads);
+        kp.blockDim = block;
         kp.sharedMemBytes = (unsigned)smem;
         kp.kernelParams = args;
         cudaGraphNode_t n;
@@ -1117,9 +1165,23 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                     rc = B.add(B.g, &prev, cla4_func(I->R, garli), cla4_grid(I, L.n), 0, args);
                 } else {
                     int S = I->S, R = I->R, tp = ns_tp;
-                    void *args[] = {&v, &L, &S, &R, &tp};
-                    rc = B.add(B.g, &prev, garli ? (void *)k_cla_ns<true> : (void *)k_cla_ns<false>,
-                               dim3((I->npat + ns_tp - 1) / ns_tp, L.n), ns_smem, args);
+                    const bool tc = tc_supported(I);
+                    const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
+                    if (ns_pat > 0) {
+                        void *args[] = {&v, &L, &S, &R, &tp};
+                        rc = B.add(B.g, &prev, garli ? (void *)k_cla_ns<true> : (void *)k_cla_ns<false>,
+                                   dim3((ns_pat + ns_tp - 1) / ns_tp, L.n), ns_smem, args);
+                    }
+                    int first = I->kpad / kTcM;
+                    const int nt = I->npat_pad / kTcM - first;
+                    if (!rc && tc && nt > 0) {
+                        size_t tsm = 0;
+                        void *f = tc_func(I->S, I->R, &tsm);
+                        void *args[] = {&v, &L, &first, &I->tc_corr};
+                        B.block = dim3(kTcM);
+                        rc = B.add(B.g, &prev, f, dim3(nt, L.n), tsm, args);
+                        B.block = dim3(kThreads);
+                    }
                 }
                 if (rc) return rc;
             }
@@ -1862,6 +1924,23 @@ int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem) {
     I->batch_tiles = tilesPerItem;
     I->batch_chunks = chunksPerItem;
     I->bgraph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_set_tensor_cores(int instance, int on) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->use_tc = on != 0;
+    I->graph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_set_tensor_core_correction(int instance, double ulps) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!(ulps >= 0.0 && ulps <= 8.0)) return GB_ERROR_OUT_OF_RANGE;
+    I->tc_corr = ulps;
+    I->graph_key = 0;
     return GB_SUCCESS;
 }
 

@@ -109,6 +109,8 @@ SIGNATURES = {
     "gb_set_batch_tuning": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "gb_get_batch_tuning": (C.c_int, [C.c_int, _I]),
     "gb_get_batch_timing": (C.c_int, [C.c_int, _D]),
+    "gb_set_tensor_cores": (C.c_int, [C.c_int, C.c_int]),
+    "gb_set_tensor_core_correction": (C.c_int, [C.c_int, C.c_double]),
     "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),
     "gbp_destroy": (C.c_int, [C.c_int]),
     "gbp_invalidate": (C.c_int, [C.c_int]),
@@ -357,6 +359,9 @@ class Instance:
 
     def synchronize(self):
         _chk(lib().gb_synchronize(self.h), "gb_synchronize")
+
+    def set_tensor_cores(self, on: bool):
+        _chk(lib().gb_set_tensor_cores(self.h, int(on)), "gb_set_tensor_cores")
 
     def set_pass_mode(self, persistent: bool):
         _chk(lib().gb_set_pass_mode(self.h, int(persistent)), "gb_set_pass_mode")

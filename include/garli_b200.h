@@ -204,6 +204,15 @@ int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 /* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
 int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
+/* precision form, 20 and 61 states: 1 (default) = CLA updates of the FP32
+ * segment on the tensor cores (tcgen05.mma kind::tf32, 3xTF32 split products,
+ * FP32 accumulation in TMEM); 0 = the CUDA-core FP64-arithmetic kernel */
+int gb_set_tensor_cores(int instance, int on);
+/* calibration of the tensor-core path: the mean loss, in ulps of the result,
+ * that one tensor-core FP32 result carries from its truncating accumulation;
+ * it is added back to every inexact K-step result (0 .. 8) */
+int gb_set_tensor_core_correction(int instance, double ulps);
+
 /* ---- batched candidate scoring and branch optimisation (4 states) ----
  * A GA generation's candidates (population.cpp:4532-4589: each mutated
  * individual is rescored, tree.cpp:4003, and the branches around its move are
