@@ -38,6 +38,7 @@ struct MEntry {
     int b1, t1, m1;
     int b2, t2, m2;
     int bk, tk, mk;
+    int wide;  // FP64 (wide) buffers: bit 0 side 1, bit 1 side 2, bit 2 the side across the branch
 };
 
 struct MixedArgs {
@@ -92,7 +93,8 @@ __device__ __forceinline__ float round_stochastic_exact(double x, unsigned int k
 // the pattern's G lanes) and its store: FP64 segment as is, FP32 segment with
 // stochastic rounding.  All G lanes of the pattern must call this together.
 template <int R>
-__device__ __forceinline__ void cla_finish_m(const View &v, int dest, int p, int r, bool act, double d[4], int m) {
+__device__ __forceinline__ void cla_finish_m(const View &v, int dest, bool wide, int p, int r, bool act, double d[4],
+                                             int m) {
     constexpr int G = Lanes<R>::G;
     double mx = act ? fmax(fmax(d[0], d[1]), fmax(d[2], d[3])) : 0.0;
 #pragma unroll
@@ -103,7 +105,9 @@ __device__ __forceinline__ void cla_finish_m(const View &v, int dest, int p, int
     const double sc = pow2d(-e);
 #pragma unroll
     for (int k = 0; k < 4; k++) d[k] *= sc;
-    if (p < v.kpad) {
+    if (wide) {
+        st4d(cla_ptr_wide(v, dest, p, R * 4) + r * 4, d);
+    } else if (p < v.kpad) {
         st4d(cla_ptr<double>(v, dest, p, R * 4) + r * 4, d);
     } else {
         float *q = cla_ptr<float>(v, dest, p, R * 4) + r * 4;
@@ -132,11 +136,27 @@ __device__ __forceinline__ void pvec_tip(const double *P, int code, double out[4
     }
 }
 
+// Child slice of category r at pattern p in FP64: a wide (FP64) buffer or
+// the FP64 segment holds doubles, the FP32 segment floats.
+template <int R>
+__device__ __forceinline__ void slice_load(const View &v, int b, bool wide, int p, int r, double c[4]) {
+    if (wide) {
+        ld4d_cg(cla_ptr_wide(v, b, p, R * 4) + r * 4, c);
+    } else if (p < v.kpad) {
+        ld4d_cg(cla_ptr<double>(v, b, p, R * 4) + r * 4, c);
+    } else {
+        const float4 a = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, b, p, R * 4) + r * 4));
+        c[0] = a.x;
+        c[1] = a.y;
+        c[2] = a.z;
+        c[3] = a.w;
+    }
+}
+
 // CLA update of tiles [t0, t1) of one op; lane = category r of pattern
 // tile * PPB + threadIdx.x / G; PL, PR = the category's P blocks in shared
-// memory.  FP32 tiles run in groups of kU with every child load of the group
-// issued before any arithmetic (memory-level parallelism); the small FP64
-// segment runs tile by tile.
+// memory.  Tiles run in groups of kU with every child load of the group
+// issued before any arithmetic (memory-level parallelism).
 constexpr int kU = 2;
 template <int R>
 __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, const double *PL, const double *PR,
@@ -144,46 +164,15 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     const int pl = threadIdx.x / G;
-    int tile = t0;
-    // FP64 segment (kpad is a multiple of 128 patterns, i.e. of whole tiles)
-    for (; tile < t1 && tile * PPB < v.kpad; tile++) {
-        const int p = tile * PPB + pl;
-        const bool act = lane_ok && p < v.npat;
-        double d[4] = {0, 0, 0, 0}, x[4], y[4];
-        int m = 0;
-        if (act) {
-            if (op.kind == kTipTip) {
-                pvec_tip(PL, v.tips[(long long)op.c1 * v.npat_pad + p], x);
-                pvec_tip(PR, v.tips[(long long)op.c2 * v.npat_pad + p], y);
-            } else {
-                double a[4];
-                ld4d_cg(cla_ptr<double>(v, op.c1, p, R * 4) + r * 4, a);
-                pvec(PL, a, x);
-                m = __ldcg(v.scalers + (long long)op.c1 * v.npat_pad + p);
-                if (op.kind == kIntInt) {
-                    double b[4];
-                    ld4d_cg(cla_ptr<double>(v, op.c2, p, R * 4) + r * 4, b);
-                    pvec(PR, b, y);
-                    m += __ldcg(v.scalers + (long long)op.c2 * v.npat_pad + p);
-                } else {
-                    pvec_tip(PR, v.tips[(long long)op.c2 * v.npat_pad + p], y);
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
-        }
-        cla_finish_m<R>(v, op.dest, p, r, act, d, m);
-    }
-    // FP32 segment, kU tiles at a time
-    for (; tile < t1; tile += kU) {
-        float4 A4[kU], B4[kU];
+    const bool w1 = op.wide & kWideC1, w2 = op.wide & kWideC2, wd = op.wide & kWideDest;
+    for (int tile = t0; tile < t1; tile += kU) {
+        double A[kU][4], B[kU][4];
         int M[kU];
         unsigned char T1[kU], T2[kU];
 #pragma unroll
         for (int u = 0; u < kU; u++) {
             const int p = (tile + u) * PPB + pl;
             const bool act = lane_ok && tile + u < t1 && p < v.npat;
-            A4[u] = B4[u] = make_float4(0.f, 0.f, 0.f, 0.f);
             M[u] = 0;
             T1[u] = T2[u] = 15;
             if (!act) continue;
@@ -192,10 +181,10 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
                 T2[u] = v.tips[(long long)op.c2 * v.npat_pad + p];
                 continue;
             }
-            A4[u] = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, op.c1, p, R * 4) + r * 4));
+            slice_load<R>(v, op.c1, w1, p, r, A[u]);
             M[u] = __ldcg(v.scalers + (long long)op.c1 * v.npat_pad + p);
             if (op.kind == kIntInt) {
-                B4[u] = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, op.c2, p, R * 4) + r * 4));
+                slice_load<R>(v, op.c2, w2, p, r, B[u]);
                 M[u] += __ldcg(v.scalers + (long long)op.c2 * v.npat_pad + p);
             } else {
                 T2[u] = v.tips[(long long)op.c2 * v.npat_pad + p];
@@ -207,35 +196,27 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
             const bool act = lane_ok && tile + u < t1 && p < v.npat;
             double d[4] = {0, 0, 0, 0}, x[4], y[4];
             if (act) {
-                if (op.kind == kTipTip) {
-                    pvec_tip(PL, T1[u], x);
-                } else {
-                    const double a[4] = {A4[u].x, A4[u].y, A4[u].z, A4[u].w};
-                    pvec(PL, a, x);
-                }
-                if (op.kind == kIntInt) {
-                    const double b[4] = {B4[u].x, B4[u].y, B4[u].z, B4[u].w};
-                    pvec(PR, b, y);
-                } else {
-                    pvec_tip(PR, T2[u], y);
-                }
+                if (op.kind == kTipTip) pvec_tip(PL, T1[u], x);
+                else pvec(PL, A[u], x);
+                if (op.kind == kIntInt) pvec(PR, B[u], y);
+                else pvec_tip(PR, T2[u], y);
 #pragma unroll
                 for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
             }
-            cla_finish_m<R>(v, op.dest, p, r, act, d, M[u]);
+            cla_finish_m<R>(v, op.dest, wd, p, r, act, d, M[u]);
         }
     }
 }
 
-// One side of a coefficient entry for lane category r at pattern p: the raw
-// child slice (FP32 segment) or tip code, loaded before any arithmetic.
+// One side of a coefficient entry for lane category r at pattern p: the child
+// slice in FP64 or the tip code, loaded before any arithmetic.
 struct SideRaw {
-    float4 c;
+    double c[4];
     int code, scale;
 };
 template <int R>
-__device__ __forceinline__ void side_load(const View &v, int b, int tip, int p, int r, SideRaw &s) {
-    s.c = make_float4(0.f, 0.f, 0.f, 0.f);
+__device__ __forceinline__ void side_load(const View &v, int b, int tip, bool wide, int p, int r, SideRaw &s) {
+    s.c[0] = s.c[1] = s.c[2] = s.c[3] = 0.0;
     s.code = 15;
     s.scale = 0;
     if (b < 0) return;
@@ -243,7 +224,7 @@ __device__ __forceinline__ void side_load(const View &v, int b, int tip, int p, 
         s.code = v.tips[(long long)b * v.npat_pad + p];
         return;
     }
-    s.c = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, b, p, R * 4) + r * 4));
+    slice_load<R>(v, b, wide, p, r, s.c);
     s.scale = __ldcg(v.scalers + (long long)b * v.npat_pad + p);
 }
 // the side's vector (P_s V_s) (or V_s itself when it has no matrix), FP64
@@ -293,60 +274,25 @@ __device__ __forceinline__ void coef_tiles_m(const View &v, const MixedArgs &A, 
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     const int pl = threadIdx.x / G;
-    int tile = t0;
-    for (; tile < t1 && tile * PPB < v.kpad; tile++) {  // FP64 segment
-        const int p = tile * PPB + pl;
-        if (!(lane_ok && p < v.npat)) continue;
-        int scale = 0;
-        double x[4], y[4] = {1, 1, 1, 1}, z[4], c[4] = {0, 0, 0, 0};
-        int code = 15;
-        if (en.t1) code = v.tips[(long long)en.b1 * v.npat_pad + p];
-        else {
-            ld4d_cg(cla_ptr<double>(v, en.b1, p, R * 4) + r * 4, c);
-            scale += __ldcg(v.scalers + (long long)en.b1 * v.npat_pad + p);
-        }
-        side_vec(c, code, en.t1, P1, x);
-        if (en.b2 >= 0) {
-            code = 15;
-            if (en.t2) code = v.tips[(long long)en.b2 * v.npat_pad + p];
-            else {
-                ld4d_cg(cla_ptr<double>(v, en.b2, p, R * 4) + r * 4, c);
-                scale += __ldcg(v.scalers + (long long)en.b2 * v.npat_pad + p);
-            }
-            side_vec(c, code, en.t2, P2, y);
-        }
-        code = 15;
-        if (en.tk) code = v.tips[(long long)en.bk * v.npat_pad + p];
-        else {
-            ld4d_cg(cla_ptr<double>(v, en.bk, p, R * 4) + r * 4, c);
-            scale += __ldcg(v.scalers + (long long)en.bk * v.npat_pad + p);
-        }
-        side_vec(c, code, en.tk, nullptr, z);
-        coef_store<R>(v, A, slot, p, r, x, y, z, scale, sU, sUi);
-    }
-    for (; tile < t1; tile += kU) {  // FP32 segment, loads of kU tiles first
+    const bool w1 = en.wide & 1, w2 = en.wide & 2, wk = en.wide & 4;
+    for (int tile = t0; tile < t1; tile += kU) {
         SideRaw S1[kU], S2[kU], SK[kU];
 #pragma unroll
         for (int u = 0; u < kU; u++) {
             const int p = (tile + u) * PPB + pl;
             const bool act = lane_ok && tile + u < t1 && p < v.npat;
-            side_load<R>(v, act ? en.b1 : -1, en.t1, p, r, S1[u]);
-            side_load<R>(v, act ? en.b2 : -1, en.t2, p, r, S2[u]);
-            side_load<R>(v, act ? en.bk : -1, en.tk, p, r, SK[u]);
+            side_load<R>(v, act ? en.b1 : -1, en.t1, w1, p, r, S1[u]);
+            side_load<R>(v, act ? en.b2 : -1, en.t2, w2, p, r, S2[u]);
+            side_load<R>(v, act ? en.bk : -1, en.tk, wk, p, r, SK[u]);
         }
 #pragma unroll
         for (int u = 0; u < kU; u++) {
             const int p = (tile + u) * PPB + pl;
             if (!(lane_ok && tile + u < t1 && p < v.npat)) continue;
             double x[4], y[4] = {1, 1, 1, 1}, z[4];
-            const double c1[4] = {S1[u].c.x, S1[u].c.y, S1[u].c.z, S1[u].c.w};
-            side_vec(c1, S1[u].code, en.t1, P1, x);
-            if (en.b2 >= 0) {
-                const double c2[4] = {S2[u].c.x, S2[u].c.y, S2[u].c.z, S2[u].c.w};
-                side_vec(c2, S2[u].code, en.t2, P2, y);
-            }
-            const double ck[4] = {SK[u].c.x, SK[u].c.y, SK[u].c.z, SK[u].c.w};
-            side_vec(ck, SK[u].code, en.tk, nullptr, z);
+            side_vec(S1[u].c, S1[u].code, en.t1, P1, x);
+            if (en.b2 >= 0) side_vec(S2[u].c, S2[u].code, en.t2, P2, y);
+            side_vec(SK[u].c, SK[u].code, en.tk, nullptr, z);
             coef_store<R>(v, A, slot, p, r, x, y, z, S1[u].scale + S2[u].scale + SK[u].scale, sU, sUi);
         }
     }
@@ -422,7 +368,7 @@ __device__ __forceinline__ void sweep_chunk(const View &v, const MixedArgs &A, i
 constexpr int kPStride = 17;
 
 template <int R>
-__global__ void __launch_bounds__(kThreads, 3) k_batch4m(View v, MixedArgs A) {
+__global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;           // patterns per CLA tile
     __shared__ double sE[8][3 * R * 4];  // one E table per warp

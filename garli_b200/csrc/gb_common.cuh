@@ -20,7 +20,10 @@ struct DevOp {
     int dest, c1, p1, c2, p2;
     int kind;
     int rescale;  // plain form: rank >= rescaleEvery (tree.cpp:3991)
+    int wide;     // precision-form batched pass: FP64 buffers, bit 0 dest, bit 1 c1, bit 2 c2
 };
+
+enum WideBits : int { kWideDest = 1, kWideC1 = 2, kWideC2 = 4 };
 
 struct LevelOps {
     int n;
@@ -60,6 +63,11 @@ template <>
 __device__ __forceinline__ float *cla_ptr<float>(const View &v, int b, int p, int RS) {
     return reinterpret_cast<float *>(v.partials + (long long)b * v.cla_bytes + (long long)v.kpad * RS * 8) +
            (long long)(p - v.kpad) * RS;
+}
+// A wide buffer b (precision form, batched pass) holds every pattern in FP64
+// and occupies the slots of buffers b and b + 1.
+__device__ __forceinline__ double *cla_ptr_wide(const View &v, int b, int p, int RS) {
+    return reinterpret_cast<double *>(v.partials + (long long)b * v.cla_bytes) + (long long)p * RS;
 }
 
 // rescale tables (tree.cpp:163-172), filled from the host with the same libm

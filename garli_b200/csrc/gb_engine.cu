@@ -66,6 +66,7 @@ struct Instance {
     double pinv = 0.0;
     int has_pinv = 0, last_const = -1;
     std::vector<int> rank;  // per CLA buffer (condlike.h rescaleRank)
+    std::vector<char> wide; // per CLA buffer: 1 = FP64 (wide, batched pass only), 2 = its second slot
     long long launches = 0;
     long long bytes = 0;
     bool site_valid = false;
@@ -435,6 +436,7 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     I->flags = I->mixed ? GB_FLAG_MIXED_FP32 : GB_FLAG_PLAIN_FP64;
     I->elem = I->mixed ? 4 : 8;
     I->rank.assign(partialsBufferCount, 0);
+    I->wide.assign(partialsBufferCount, 0);
     I->h_rates.assign(categoryCount, 1.0);
     // FP64 segment: everything in the plain form; in the precision form room for
     // max(128, npat/32) heavy patterns (rounded to the 128-pattern tile)
@@ -777,7 +779,7 @@ namespace gb {
 // rule (tree.cpp:7665-8598) to the instance's rank table as the ops would
 // execute and returns the per-level device op lists.
 static int prepare_ops(Instance *I, const gb_cla_operation *ops, int count, int rescaleEvery,
-                       std::vector<std::vector<DevOp>> &levels) {
+                       std::vector<std::vector<DevOp>> &levels, bool allow_wide = false) {
     levels.clear();
     if (count <= 0) return GB_SUCCESS;
     std::vector<int> order(count);
@@ -820,6 +822,16 @@ static int prepare_ops(Instance *I, const gb_cla_operation *ops, int count, int 
         d.dest = dest;
         d.c1 = is_cla(c1) ? c1 - nt : c1;
         d.c2 = is_cla(c2) ? c2 - nt : c2;
+        d.wide = 0;
+        {
+            const char wd = I->wide[dest], w1 = is_cla(c1) ? I->wide[c1 - nt] : 0, w2 = is_cla(c2) ? I->wide[c2 - nt] : 0;
+            if (wd == 2 || w1 == 2 || w2 == 2) return GB_ERROR_OUT_OF_RANGE;  // the second slot of a wide buffer
+            d.wide = (wd ? kWideDest : 0) | (w1 ? kWideC1 : 0) | (w2 ? kWideC2 : 0);
+            if (d.wide && !allow_wide) {
+                g_last_error = "FP64 (wide) buffers are read and written by gb_batch_newton only";
+                return GB_ERROR_NO_IMPLEMENTATION;
+            }
+        }
         d.p1 = p1;
         d.p2 = p2;
         d.rescale = (!I->mixed && rank >= rescaleEvery) ? 1 : 0;
@@ -947,6 +959,15 @@ int gb_get_partials(int instance, int bufferIndex, double *out) {
     GB_CUDA(cudaStreamSynchronize(I->stream));
     const double *d64 = reinterpret_cast<const double *>(raw.data());
     const float *d32 = reinterpret_cast<const float *>(raw.data() + (size_t)I->kpad * RS * 8);
+    if (I->wide[b] == 1) {  // FP64 throughout, over two buffer slots
+        std::vector<double> wraw((size_t)I->npat * RS);
+        GB_CUDA(cudaMemcpyAsync(wraw.data(), (const char *)I->d_partials + (size_t)b * I->cla_bytes,
+                                wraw.size() * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        for (int q = 0; q < I->npat; q++)
+            std::memcpy(out + (size_t)I->perm[q] * RS, wraw.data() + (size_t)q * RS, RS * sizeof(double));
+        return GB_SUCCESS;
+    }
     for (int q = 0; q < I->npat; q++) {
         double *dst = out + (size_t)I->perm[q] * RS;
         for (int k = 0; k < RS; k++)
@@ -1711,8 +1732,8 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         g_last_error = "gb_batch_newton: 4-state data only";
         return GB_ERROR_NO_IMPLEMENTATION;
     }
-    if (opCount < 0 || stepOpCount < 0 || candidateCount < 1 || stepsPerCandidate < 1 || !(precision > 0.0) ||
-        !(minLength > 0.0) || !(maxLength > minLength) || !steps || !out)
+    if (opCount < 0 || stepOpCount < 0 || candidateCount < 0 || stepsPerCandidate < 1 || !(precision > 0.0) ||
+        !(minLength > 0.0) || !(maxLength > minLength) || (candidateCount > 0 && (!steps || !out)))
         return GB_ERROR_OUT_OF_RANGE;
     const int nC = candidateCount, K = stepsPerCandidate;
     for (int i = 0; i < nC * K; i++) {
@@ -1726,7 +1747,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
     const std::vector<int> rank_before = I->rank;
     BatchPlan P;
     std::vector<std::vector<DevOp>> levels;
-    int rc = prepare_ops(I, ops, opCount, rescaleEvery, levels);
+    int rc = prepare_ops(I, ops, opCount, rescaleEvery, levels, I->mixed);
     unsigned long long key = 1469598103934665603ULL;
     auto add_level = [&](const std::vector<DevOp> &lv) {
         BCmd c;
@@ -1739,7 +1760,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
     };
     if (rc == GB_SUCCESS)
         for (auto &lv : levels) add_level(lv);
-    for (int k = 0; k < K && rc == GB_SUCCESS && I->mixed; k++) {
+    for (int k = 0; k < K && rc == GB_SUCCESS && I->mixed && nC > 0; k++) {
         // precision form: the step's partial is formed inside the coefficient pass
         BCmd cc;
         cc.type = kBCoef;
@@ -1749,6 +1770,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
             tip = b < I->ntip;
             idx = tip ? b : b - I->ntip;
         };
+        auto is_wide = [&](int idx, int tip) { return !tip && idx >= 0 && I->wide[idx] == 1; };
         for (int c = 0; c < nC; c++) {
             const gb_batch_step &s = steps[c * K + k];
             MEntry m;
@@ -1771,6 +1793,10 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
             }
             side(s.childIndex, m.bk, m.tk);
             m.mk = s.transMatIndex;
+            m.wide = (is_wide(m.b1, m.t1) ? 1 : 0) | (is_wide(m.b2, m.t2) ? 2 : 0) | (is_wide(m.bk, m.tk) ? 4 : 0);
+            if ((m.b1 >= 0 && !m.t1 && I->wide[m.b1] == 2) || (m.b2 >= 0 && !m.t2 && I->wide[m.b2] == 2) ||
+                (!m.tk && I->wide[m.bk] == 2))
+                rc = GB_ERROR_OUT_OF_RANGE;
             P.mentries.push_back(m);
         }
         P.cmds.push_back(cc);
@@ -1779,7 +1805,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         P.cmds.push_back(nc);
     }
     if (I->mixed) key = fnv(key, P.mentries.data(), sizeof(MEntry) * P.mentries.size());
-    for (int k = 0; k < K && rc == GB_SUCCESS && !I->mixed; k++) {
+    for (int k = 0; k < K && rc == GB_SUCCESS && !I->mixed && nC > 0; k++) {
         std::vector<gb_cla_operation> sops;
         for (int c = 0; c < nC; c++)
             if (steps[c * K + k].claOp >= 0) {
@@ -1788,7 +1814,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
                 sops.push_back(o);
             }
         std::vector<std::vector<DevOp>> sl;
-        rc = prepare_ops(I, sops.data(), (int)sops.size(), rescaleEvery, sl);
+        rc = prepare_ops(I, sops.data(), (int)sops.size(), rescaleEvery, sl, false);
         if (rc) break;
         for (auto &lv : sl) add_level(lv);
         BCmd nc;
@@ -1810,11 +1836,13 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         I->rank = rank_before;
         return rc;
     }
-    BCmd fs;  // lnL of every candidate at its optimised lengths
-    fs.type = kBScore;
-    fs.a = (K - 1) * nC;
-    fs.b = nC;
-    P.cmds.push_back(fs);
+    if (nC > 0) {
+        BCmd fs;  // lnL of every candidate at its optimised lengths
+        fs.type = kBScore;
+        fs.a = (K - 1) * nC;
+        fs.b = nC;
+        P.cmds.push_back(fs);
+    }
     P.max_entries = nC;
     key = fnv(key, P.entries.data(), sizeof(BEntry) * P.entries.size());
     key = fnv(key, P.cmds.data(), sizeof(BCmd) * P.cmds.size());
@@ -1860,19 +1888,27 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         GB_CUDA(cudaMemcpyAsync(I->d_mentries, P.mentries.data(), P.mentries.size() * sizeof(MEntry),
                                 cudaMemcpyHostToDevice, I->stream));
     NrParams prm{precision, minLength, maxLength};
-    if (I->batch_tiles == 0 || I->batch_chunks == 0) {
-        if ((rc = autotune_batch(I, P, prm, rescaleEvery))) {
-            I->rank = rank_before;
-            return rc;
+    int tiles = I->batch_tiles, chunks = I->batch_chunks;
+    if (tiles == 0 || chunks == 0) {
+        if (nC > 0) {
+            if ((rc = autotune_batch(I, P, prm, rescaleEvery))) {
+                I->rank = rank_before;
+                return rc;
+            }
+            tiles = I->batch_tiles;
+            chunks = I->batch_chunks;
+        } else {  // levels only (a base tree): not worth tuning for
+            tiles = I->mixed ? 16 : 4;
+            chunks = 1;
         }
     }
     cudaEvent_t te0 = nullptr, te1 = nullptr;
-    if (I->timing) {
+    if (I->timing && nC > 0) {
         cudaEventCreate(&te0);
         cudaEventCreate(&te1);
         cudaEventRecord(te0, I->stream);
     }
-    if ((rc = enqueue_batch(I, P, prm, rescaleEvery, I->batch_tiles, I->batch_chunks, true))) {
+    if ((rc = enqueue_batch(I, P, prm, rescaleEvery, tiles, chunks, nC > 0))) {
         I->rank = rank_before;
         return rc;
     }
@@ -1932,6 +1968,24 @@ int gb_set_tensor_cores(int instance, int on) {
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
     I->use_tc = on != 0;
     I->graph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_set_buffer_precision(int instance, int bufferIndex, int fp64) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!I->mixed) return GB_ERROR_NO_IMPLEMENTATION;  // the plain form is FP64 throughout
+    const int b = bufferIndex - I->ntip;
+    if (b < 0 || b + 1 >= I->nbuf) return GB_ERROR_OUT_OF_RANGE;
+    if (fp64) {
+        if (I->wide[b] == 2 || I->wide[b + 1] == 1) return GB_ERROR_OUT_OF_RANGE;
+        I->wide[b] = 1;
+        I->wide[b + 1] = 2;
+    } else if (I->wide[b] == 1) {
+        I->wide[b] = 0;
+        I->wide[b + 1] = 0;
+    }
+    I->version++;
     return GB_SUCCESS;
 }
 

@@ -138,6 +138,9 @@ struct Pop {
     std::unordered_map<uint64_t, int> mat_of;  // length bits -> matrix slot
     int base_mats = 0, next_mat = 0;
     std::vector<double> mat_len;
+    bool wide_alloc = false;       // new CLAs of the base tree go to FP64 (two-slot) buffers
+    int base_mode = -1;            // the mode the base tree was prepared for: 1 batched, 0 per-tree
+    std::vector<int> wide_bufs;    // buffers currently marked FP64
     long long c_ops = 0, c_updates = 0, c_evals = 0, c_base_ops = 0, c_edges = 0;
     double c_bytes = 0.0;
     int npat = 0;
@@ -205,12 +208,18 @@ Made need_key(Pop &p, const Topo &t, int v, int u, std::vector<gb_cla_operation>
     const Key key = combine(term(a.key, cl[0]), term(b.key, cl[1]));
     auto it = p.cla.find(key);
     if (it != p.cla.end()) return {key, it->second};
-    if (p.next_buf >= p.ntip + p.nbuf) {
+    const int slots = p.wide_alloc ? 2 : 1;
+    if (p.next_buf + slots > p.ntip + p.nbuf) {
         *rc = GB_ERROR_OUT_OF_RANGE;
         return {key, {0, 0}};
     }
     Cla made;
-    made.buf = p.next_buf++;
+    made.buf = p.next_buf;
+    p.next_buf += slots;
+    if (p.wide_alloc) {
+        if ((*rc = gb_set_buffer_precision(p.inst, made.buf, 1))) return {key, {0, 0}};
+        p.wide_bufs.push_back(made.buf);
+    }
     made.level = (a.cla.level > b.cla.level ? a.cla.level : b.cla.level) + 1;
     gb_cla_operation op;
     op.destClaIndex = made.buf;
@@ -224,12 +233,18 @@ Made need_key(Pop &p, const Topo &t, int v, int u, std::vector<gb_cla_operation>
     return {key, made};
 }
 
-// every directional CLA of the base tree, computed once and kept
-int prepare_base(Pop &p) {
+// every directional CLA of the base tree, computed once and kept.  wide: in
+// FP64 buffers (precision form, batched pass) -- they are shared by every
+// candidate, so their storage error would otherwise enter every candidate's lnL.
+int prepare_base(Pop &p, bool wide) {
     p.cla.clear();
     p.mat_of.clear();
     p.next_buf = p.ntip;
     p.next_mat = 0;
+    for (int b : p.wide_bufs) gb_set_buffer_precision(p.inst, b, 0);
+    p.wide_bufs.clear();
+    // a plain instance is FP64 throughout and has no FP64 buffer option
+    p.wide_alloc = wide && p.nbuf >= 2 && gb_set_buffer_precision(p.inst, p.ntip, 0) == GB_SUCCESS;
     std::vector<gb_cla_operation> ops;
     int rc = GB_SUCCESS;
     const Topo &t = p.base;
@@ -240,13 +255,23 @@ int prepare_base(Pop &p) {
         const int k = t.nbrs(v, nb, ln);
         for (int i = 0; i < k && !rc; i++) need_key(p, t, v, nb[i], ops, &rc);
     }
+    const bool wide_base = p.wide_alloc;
+    p.wide_alloc = false;
     if (rc) return rc;
     p.base_bufs = p.next_buf;
     p.base_mats = p.next_mat;
     std::vector<gb_transmat_operation> tops;
     for (int m = 0; m < p.next_mat; m++) tops.push_back({m, p.mat_len[m], 0, 1});
     if ((rc = gb_update_transition_matrices(p.inst, tops.data(), (int)tops.size()))) return rc;
-    if ((rc = gb_update_partials(p.inst, ops.data(), (int)ops.size(), p.rescaleEvery))) return rc;
+    if (wide_base) {
+        // CLA updates only, by the batched kernel (the one that reads and writes FP64 buffers)
+        if ((rc = gb_batch_newton(p.inst, ops.data(), (int)ops.size(), nullptr, 0, nullptr, 0, 1, p.rescaleEvery,
+                                  0.01, p.minBrlen, p.maxBrlen, nullptr)))
+            return rc;
+    } else if ((rc = gb_update_partials(p.inst, ops.data(), (int)ops.size(), p.rescaleEvery))) {
+        return rc;
+    }
+    p.base_mode = wide ? 1 : 0;
     // every level of the base is computed: its CLAs have level 0 from now on
     for (auto &kv : p.cla) kv.second.level = 0;
     p.c_base_ops += (long long)ops.size();
@@ -458,7 +483,9 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
         return GB_ERROR_OUT_OF_RANGE;
     for (int attempt = 0;; attempt++) {
         int rc = GB_SUCCESS;
-        if (!p->base_ready) rc = prepare_base(*p);
+        // the batched precision form keeps the base tree in FP64 buffers, the per-tree path cannot read them
+        if (p->base_ready && (p->base_mode == 1) != (sequential == 0)) p->base_ready = false;
+        if (!p->base_ready) rc = prepare_base(*p, sequential == 0);
         if (rc) return rc;
         reset_call(*p);
         Plan P;

@@ -111,6 +111,7 @@ SIGNATURES = {
     "gb_get_batch_timing": (C.c_int, [C.c_int, _D]),
     "gb_set_tensor_cores": (C.c_int, [C.c_int, C.c_int]),
     "gb_set_tensor_core_correction": (C.c_int, [C.c_int, C.c_double]),
+    "gb_set_buffer_precision": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),
     "gbp_destroy": (C.c_int, [C.c_int]),
     "gbp_invalidate": (C.c_int, [C.c_int]),
@@ -504,7 +505,7 @@ def population_engine(pd, child3, dlen, model: Model, ncand: int, device=0, mixe
     """Instance + Population sized for ``ncand`` candidates of a base tree."""
     ntax = pd.ntax
     nnodes = 2 * ntax - 2
-    nbuf = 3 * (ntax - 2) + ncand * (extra_bufs_per_cand + 1)
+    nbuf = 6 * (ntax - 2) + ncand * (extra_bufs_per_cand + 1)  # base CLAs may take two slots (FP64)
     nmat = nnodes + ncand * 8
     inst = Instance(ntax, nbuf, pd.nstates, pd.npat, model.ncat, nmat, device=device, mixed=mixed)
     inst.set_data(pd)

@@ -228,7 +228,9 @@ int gb_set_tensor_core_correction(int instance, double ulps);
  * lockstep; the matrices hold the optimised P(t) on return.
  * out[4c .. 4c+3] = lnL at the starting lengths (the candidate's rescore),
  * lnL at the optimised lengths, summed estimated improvement, derivative
- * evaluations.  Work-item sizes are autotuned on the first call. */
+ * evaluations.  Work-item sizes are autotuned on the first call with
+ * candidates.  candidateCount = 0 runs the CLA updates only (e.g. a parent
+ * tree's CLAs into FP64 buffers, gb_set_buffer_precision). */
 typedef struct {
     int claOp;
     int partialIndex;
@@ -238,6 +240,12 @@ typedef struct {
 int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, const gb_cla_operation *stepOps,
                     int stepOpCount, const gb_batch_step *steps, int candidateCount, int stepsPerCandidate,
                     int rescaleEvery, double precision, double minLength, double maxLength, double *out);
+/* precision form: store CLA buffer bufferIndex in FP64 for every pattern (1) or
+ * in the instance's FP64/FP32 segments (0).  An FP64 buffer occupies its own
+ * slot and the next one (bufferIndex + 1 must be left unused); it is read and
+ * written by gb_batch_newton only (and read back by gb_get_partials).  For CLAs
+ * many candidates share, such as a GA generation's parent tree. */
+int gb_set_buffer_precision(int instance, int bufferIndex, int fp64);
 /* work-item sizes: CLA tiles (64 patterns at 4 categories) and edge chunks
  * (256 patterns) per CTA work item; 0, 0 = autotune on the next call */
 int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem);
