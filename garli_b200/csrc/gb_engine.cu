@@ -24,6 +24,7 @@
 #include "gb_newton_dna.cuh"
 #include "gb_nstate.cuh"
 #include "gb_persist.cuh"
+#include "gb_persist_mixed.cuh"
 #include "gb_pmat.cuh"
 #include "gb_tc.cuh"
 
@@ -293,8 +294,21 @@ static int set_smem_attrs() {
 }
 
 static void *pass4_func(int R, bool garli) {
+    // precision form: its own kernel (gb_persist_mixed.cuh)
+    if (!garli) {
+        switch (R) {
+            case 1: return (void *)k_pass4m<1>;
+            case 2: return (void *)k_pass4m<2>;
+            case 3: return (void *)k_pass4m<3>;
+            case 4: return (void *)k_pass4m<4>;
+            case 5: return (void *)k_pass4m<5>;
+            case 6: return (void *)k_pass4m<6>;
+            case 7: return (void *)k_pass4m<7>;
+            default: return (void *)k_pass4m<8>;
+        }
+    }
 #define GB_CASE(r) \
-    case r: return garli ? (void *)k_pass4<r, true> : (void *)k_pass4<r, false>;
+    case r: return (void *)k_pass4<r, true>;
     switch (R) {
         GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
     }

@@ -207,10 +207,13 @@ def test_abi_operation_lists_directly():
 
 @pytest.mark.parametrize("mixed", [False, True])
 def test_device_newton_pass_equals_host_pass(mixed):
-    """The persistent-kernel pass and the graph pass take exactly the host driver's
-    Newton decisions (same partition of the pattern sums, same gb::nr_step)."""
+    """The graph pass takes exactly the host driver's Newton decisions (same
+    partition of the pattern sums, same gb::nr_step); so does the persistent
+    pass of the plain form.  The precision form's persistent pass has its own
+    fused arithmetic (k_pass4m): there the optimised lengths agree to 1e-3
+    relative and the rescored lnL to the precision form's bar."""
     w = synth.make_dna(40, 3000, seed=21, pinv_range=(0.05, 0.3))
-    res = []
+    res = {}
     for mode in ("persistent", "graph", "host"):
         inst, tree = engine.tree_engine(w.data, w.child3, w.dlen * 1.3, w.model, mixed=mixed)
         inst.set_pass_mode(mode == "persistent")
@@ -219,12 +222,18 @@ def test_device_newton_pass_equals_host_pass(mixed):
         imp, _ = tree.optimize_all_branches(0.01)
         bl = tree.branch_lengths()
         tree.make_all_dirty()
-        res.append((bl, tree.score(0), imp))
+        res[mode] = (bl, tree.score(0), imp)
         tree.close()
         inst.close()
-    for bl, lnl, imp in res[1:]:
-        assert np.array_equal(res[0][0], bl), np.abs(res[0][0] - bl).max()
-        assert res[0][1] == lnl and res[0][2] == imp
+    exact = ["graph", "persistent"] if not mixed else ["graph"]
+    for m in exact:
+        bl, lnl, imp = res[m]
+        assert np.array_equal(res["host"][0], bl), (m, np.abs(res["host"][0] - bl).max())
+        assert res["host"][1] == lnl and res["host"][2] == imp
+    if mixed:
+        bl, lnl, imp = res["persistent"]
+        assert np.allclose(bl, res["host"][0], rtol=1e-3, atol=1e-8)
+        assert abs(lnl - res["host"][1]) <= 1e-4 * max(1.0, w.data.npat / 2000)
 
 
 def test_device_newton_pass_matches_oracle_and_is_repeatable():
