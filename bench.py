@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--no-single", action="store_true", help="skip the single-tree secondary measurement")
     ap.add_argument("--batch-only", action="store_true",
                     help="profiling: only the batched form (no per-tree comparison, no e2e pass)")
+    ap.add_argument("--nstate-only", action="store_true",
+                    help="profiling: only the 20- and 61-state rescores (tensor cores, CUDA cores, plain)")
+    ap.add_argument("--single-only", action="store_true",
+                    help="profiling: only the 128x100k single-tree step (precision and plain forms)")
     ap.add_argument("--cpu-sample-cands", type=int, default=24, help="candidates in the CPU baseline sample")
     ap.add_argument("--cpu-repeats", type=int, default=16, help="timed repeats per sampled candidate")
     ap.add_argument("--ref-cands-per-step", type=int, default=2, help="candidates per --impl reference step")
@@ -497,6 +501,22 @@ def main():
     device = local if ws > 1 else 0
     torch.cuda.set_device(device)
     peak, peak_kind = peaks()
+    if args.single_only:
+        res = single_tree(args, device, rank)
+        if rank == 0:
+            print(json.dumps({"single_only": True, "single_tree": res}))
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    if args.nstate_only:
+        res = {"aa_20_states": nstate_forms("aa", device), "codon_61_states": nstate_forms("codon", device)}
+        if rank == 0:
+            print(json.dumps({"nstate_only": True, "nstate": res}))
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     bw = batch_workload(args, seed=4 + rank)
     w, c3s, dls, conn = bw
 

@@ -354,18 +354,21 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
 }
 
 // Algorithmic device-memory bytes of one batched pass of the precision form
-// per pattern (R = 4 categories, FP32 CLAs): see gbp_get_counters.
+// per pattern (R = 4 categories): a CLA read is 64 B + a 4 B scaler (FP32),
+// 128 + 4 B when it is an FP64 parent-tree buffer, 1 B for a tip; a CLA
+// update writes 64 + 4 B; a coefficient pattern writes 128 + 4 B; an edge
+// evaluation pattern reads 128 + 4 + 4 + 4 B (coefficients, scale, count,
+// constant state).  See gbp_get_counters.
 double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps) {
-    auto is_tip = [&](int b) { return b < p.ntip; };
+    auto side = [&](int b) {
+        if (b < p.ntip) return 1.0;
+        return (p.base_mode == 1 && !p.wide_bufs.empty() && b < p.base_bufs) ? 132.0 : 68.0;
+    };
     double per = 0.0;
-    for (const gb_cla_operation &o : P.ops) {
-        const int t = (is_tip(o.childClaIndex1) ? 1 : 0) + (is_tip(o.childClaIndex2) ? 1 : 0);
-        per += t == 0 ? 204.0 : t == 1 ? 137.0 : 70.0;
-    }
+    for (const gb_cla_operation &o : P.ops) per += side(o.childClaIndex1) + side(o.childClaIndex2) + 68.0;
     for (int i = 0; i < 3 * nC; i++) {
         const gb_cla_operation &o = P.step_ops[i];
-        per += 132.0;
-        for (int b : {o.childClaIndex1, o.childClaIndex2, P.steps[i].childIndex}) per += is_tip(b) ? 1.0 : 68.0;
+        per += 132.0 + side(o.childClaIndex1) + side(o.childClaIndex2) + side(P.steps[i].childIndex);
     }
     per += 140.0 * (double)sweeps;
     return per * (double)p.npat;

@@ -4,7 +4,8 @@
 // Per rate category r the update is two dense products followed by an
 // element-wise one (Tree::CalcFullCLAInternalInternalNState, tree.cpp:7843):
 //     dest[p, r, i] = (sum_j P1_r[i][j] L[p, r, j]) * (sum_j P2_r[i][j] R[p, r, j]).
-// A CTA takes 128 patterns of one op.  Each product is a 128 x 32 x K UMMA
+// A CTA takes 128 patterns of one op, one child at a time with as many rate
+// categories per round as TMEM holds.  Each product is a 128 x 32 x K UMMA
 // per 32-state half (M = patterns, K = states padded to 24 / 64) issued by one
 // thread with tcgen05.mma kind::tf32, operands in shared memory (K-major, no
 // swizzle), results in TMEM.  Operands are split x = hi + lo with hi = tf32(x),
@@ -86,6 +87,13 @@ __device__ __forceinline__ void tc_ld8(uint32_t taddr, float v[8]) {
     for (int j = 0; j < 8; j++) v[j] = __uint_as_float(r[j]);
 }
 
+__device__ __forceinline__ void tc_ld8_nw(uint32_t taddr, uint32_t r[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
 // bounded wait for the phase with the given parity; false on timeout
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     for (long long it = 0; it < (1LL << 24); it++) {
@@ -108,6 +116,7 @@ __device__ __forceinline__ void tc_stage_a(const View &v, int child, bool tip, i
                                            unsigned char *lo) {
     constexpr int KP = TcShape<S>::KP;
     const float *src = tip ? nullptr : cla_ptr<float>(v, child, p0, R * S);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < kTcM * KP; idx += blockDim.x) {
         const int m = idx / KP, k = idx % KP;
         const int p = p0 + m;
@@ -147,13 +156,19 @@ __device__ __forceinline__ void tc_stage_b(const View &v, int mat, int r, unsign
 template <int S, int R>
 struct TcSmem {
     static constexpr int KP = TcShape<S>::KP, NP = TcShape<S>::NP;
-    static constexpr int KB = KP / 8;          // K steps
-    static constexpr int NH = NP / 32;         // 32-state halves of N
+    static constexpr int KB = KP / 8;            // K steps
+    static constexpr int NH = NP / 32;           // 32-state halves of N
+    static constexpr int RCOLS = (KB + 1) * 32;  // TMEM columns of one (category, half): K-step regions + cross terms
     static constexpr int A_BYTES = kTcM * KP * 4, B_BYTES = NP * KP * 4;
     static constexpr int RSP = R * S + 1;  // product row stride (odd: no bank conflicts between rows)
     static constexpr int PROD_BYTES = kTcM * RSP * 8;
-    static constexpr int BYTES = 2 * A_BYTES + 2 * B_BYTES + PROD_BYTES;
-    static constexpr int COLS_USED = (KB + 1) * 32;  // one region per K step + the cross terms
+    // categories per round.  Measured on B200 (20 states, 4 categories): one
+    // category per round at 2 CTAs/SM beats four per round at 1 CTA/SM (4.35 vs
+    // 6.37 ms per rescore): the staging and FP64 epilogue around the UMMAs are
+    // latency-bound and need the second CTA to hide it.
+    static constexpr int RG = 1;
+    static constexpr int BYTES = RG * (2 * A_BYTES + 2 * B_BYTES) + PROD_BYTES;
+    static constexpr int COLS_USED = RG * RCOLS;
     static constexpr int COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
                                 : COLS_USED <= 256 ? 256 : 512;
 };
@@ -165,16 +180,17 @@ __device__ __forceinline__ double ulp_f(float f) {
 }
 
 // One CTA = 128 patterns [first_tile*128 + blockIdx.x*128, +128) of op blockIdx.y.
+// A round = one child, RG categories, one 32-state half: stage, issue, wait,
+// read back.
 template <int S, int R>
 __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int first_tile, double corr_ulps) {
     using SM = TcSmem<S, R>;
-    constexpr int KP = SM::KP, KB = SM::KB, NH = SM::NH;
+    constexpr int KP = SM::KP, KB = SM::KB, NH = SM::NH, RG = SM::RG;
+    constexpr int GB = 2 * SM::A_BYTES + 2 * SM::B_BYTES;  // staging bytes of one category
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ __align__(8) unsigned long long s_mbar;
     __shared__ uint32_t s_taddr;
-    unsigned char *Ah = tc_smem, *Al = Ah + SM::A_BYTES;
-    unsigned char *Bh = Al + SM::A_BYTES, *Bl = Bh + SM::B_BYTES;
-    double *prod = reinterpret_cast<double *>(Bl + SM::B_BYTES);  // [128][RSP]
+    double *prod = reinterpret_cast<double *>(tc_smem + RG * GB);  // [128][RSP]
     const DevOp op = ops.op[blockIdx.y];
     const int p0 = (first_tile + blockIdx.x) * kTcM;
     const int warp = threadIdx.x >> 5;
@@ -199,30 +215,40 @@ __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int fi
     const uint32_t sbo = KP * 32, lbo = 128;
     bool ok = true;
     uint32_t phase = 0;
-    for (int r = 0; r < R && ok; r++) {
-        for (int c = 0; c < 2 && ok; c++) {
-            const int child = c ? op.c2 : op.c1;
-            const bool tip = c ? op.kind != kIntInt : op.kind == kTipTip;
-            tc_stage_a<S, R>(v, child, tip, p0, r, Ah, Al);
-            tc_stage_b<S, R>(v, c ? op.p2 : op.p1, r, Bh, Bl);
+    for (int c = 0; c < 2 && ok; c++) {
+        const int child = c ? op.c2 : op.c1;
+        const bool tip = c ? op.kind != kIntInt : op.kind == kTipTip;
+        // a row is exact (no truncation to correct) when it is a one-hot tip state
+        bool exact_row = false;
+        if (tip && p < v.npat) exact_row = v.tips[(long long)child * v.npat_pad + p] < S;
+        for (int r0 = 0; r0 < R && ok; r0 += RG) {
+            const int ng = min(RG, R - r0);
+            for (int g = 0; g < ng; g++) {
+                unsigned char *base = tc_smem + g * GB;
+                tc_stage_a<S, R>(v, child, tip, p0, r0 + g, base, base + SM::A_BYTES);
+                tc_stage_b<S, R>(v, c ? op.p2 : op.p1, r0 + g, base + 2 * SM::A_BYTES,
+                                 base + 2 * SM::A_BYTES + SM::B_BYTES);
+            }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // a row is exact (no truncation to correct) when it is a one-hot tip state
-            bool exact_row = false;
-            if (tip && p < v.npat) exact_row = v.tips[(long long)child * v.npat_pad + p] < S;
             for (int h = 0; h < NH && ok; h++) {
                 if (threadIdx.x == 0) {
                     // B rows [32h, 32h+32) = 8-row groups 4h .. 4h+3, each SBO bytes apart
                     const uint32_t hoff = (uint32_t)h * 4 * sbo;
-                    for (int kb = 0; kb < KB; kb++) {
-                        const uint32_t o = kb * 256;
-                        const uint64_t ah = umma_desc(smem_u32(Ah) + o, lbo, sbo), al = umma_desc(smem_u32(Al) + o, lbo, sbo);
-                        const uint64_t bh = umma_desc(smem_u32(Bh) + hoff + o, lbo, sbo);
-                        const uint64_t bl = umma_desc(smem_u32(Bl) + hoff + o, lbo, sbo);
-                        tc_mma(taddr + kb * 32, ah, bh, idesc, 0);       // main term, own region
-                        tc_mma(taddr + KB * 32, ah, bl, idesc, kb > 0);  // cross terms, accumulated
-                        tc_mma(taddr + KB * 32, al, bh, idesc, 1);
+                    for (int g = 0; g < ng; g++) {
+                        const uint32_t sa = smem_u32(tc_smem + g * GB);
+                        const uint32_t ahb = sa, alb = sa + SM::A_BYTES;
+                        const uint32_t bhb = sa + 2 * SM::A_BYTES + hoff, blb = bhb + SM::B_BYTES;
+                        const uint32_t dbase = taddr + (uint32_t)(g * SM::RCOLS);
+                        for (int kb = 0; kb < KB; kb++) {
+                            const uint32_t o = kb * 256;
+                            const uint64_t ah = umma_desc(ahb + o, lbo, sbo), al = umma_desc(alb + o, lbo, sbo);
+                            const uint64_t bh = umma_desc(bhb + o, lbo, sbo), bl = umma_desc(blb + o, lbo, sbo);
+                            tc_mma(dbase + kb * 32, ah, bh, idesc, 0);       // main term, own region
+                            tc_mma(dbase + KB * 32, ah, bl, idesc, kb > 0);  // cross terms, accumulated
+                            tc_mma(dbase + KB * 32, al, bh, idesc, 1);
+                        }
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                                  : "memory");
@@ -233,27 +259,31 @@ __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int fi
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 if (!ok) break;
                 // (P_c V_c)_s for s in [32h, 32h+32): FP64 sum of the K-step regions
-                for (int c8 = 0; c8 < 32; c8 += 8) {
-                    double val[8];
-                    float t[8];
-                    tc_ld8(trow + KB * 32 + c8, t);
+                for (int g = 0; g < ng; g++) {
+                    const uint32_t rbase = trow + (uint32_t)(g * SM::RCOLS);
+                    const int r = r0 + g;
+                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                        uint32_t t[KB + 1][8];
 #pragma unroll
-                    for (int j = 0; j < 8; j++) val[j] = (double)t[j];
-                    for (int kb = 0; kb < KB; kb++) {
-                        tc_ld8(trow + kb * 32 + c8, t);
+                        for (int kb = 0; kb <= KB; kb++) tc_ld8_nw(rbase + kb * 32 + c8, t[kb]);
+                        tc_wait_ld();
 #pragma unroll
-                        for (int j = 0; j < 8; j++) val[j] += (double)t[j] + (exact_row ? 0.0 : corr_ulps * ulp_f(t[j]));
-                    }
+                        for (int j = 0; j < 8; j++) {
+                            double val = (double)__uint_as_float(t[KB][j]);
 #pragma unroll
-                    for (int j = 0; j < 8; j++) {
-                        const int st = h * 32 + c8 + j;
-                        if (st < S) {
-                            double *q = prod + (long long)m * SM::RSP + r * S + st;
-                            *q = c ? *q * val[j] : val[j];
+                            for (int kb = 0; kb < KB; kb++) {
+                                const float f = __uint_as_float(t[kb][j]);
+                                val += (double)f + (exact_row ? 0.0 : corr_ulps * ulp_f(f));
+                            }
+                            const int st = h * 32 + c8 + j;
+                            if (st < S) {
+                                double *q = prod + (long long)m * SM::RSP + r * S + st;
+                                *q = c ? *q * val : val;
+                            }
                         }
                     }
                 }
-                // the next round's MMAs overwrite TMEM: every read above is complete
+                // the next round's MMAs overwrite TMEM and shared memory: every read above is complete
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncthreads();
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

@@ -282,9 +282,10 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
 /* last call: [0] CLA updates (the per-step partials included), [1] pattern-updates,
  * [2] derivative evaluations, [4] edge evaluations (derivative evaluations + the
  * final scores), [5] algorithmic device-memory bytes of the precision form's
- * batched pass (FP32 CLAs: 204 / 137 / 70 B per int-int / int-tip / tip-tip
- * pattern-update, 132 B written + 68 B per CLA side read per coefficient
- * pattern, 140 B per edge-evaluation pattern); [3] base-tree CLA updates since creation */
+ * batched pass, per pattern at 4 categories: a CLA read 68 B (FP32 + scaler),
+ * 132 B for an FP64 parent-tree CLA, 1 B for a tip; 68 B per CLA update
+ * written; 132 B per coefficient pattern written; 140 B per edge-evaluation
+ * pattern; [3] base-tree CLA updates since creation */
 int gbp_get_counters(int pop, long long *out6);
 
 /* ---- edge evaluation without device allocation ----
