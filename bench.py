@@ -544,16 +544,9 @@ def main():
     torch.cuda.synchronize(device)
     if pg:
         pg.barrier()
-    ms = mixed["ms"]
-    updates = float(mixed["updates"])
-    edges = float(mixed["edges"])
-    if pg:
-        t = torch.tensor([ms], dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-        u = torch.tensor([updates, edges], dtype=torch.float64)
-        pg.all_reduce(u)
-        updates, edges = float(u[0]), float(u[1])
+    from garli_b200.replicas import aggregate
+
+    ms, (updates, edges) = aggregate(pg, mixed["ms"], [mixed["updates"], mixed["edges"]])
     value = updates / (ms / 1000.0)
     plain_v = plain["updates"] / (plain["ms"] / 1000.0)
     mixed["bw"] = bw
@@ -567,10 +560,7 @@ def main():
         f["pop"].close()
         f["inst"].close()
     e2e_v, bi, bo = e2e_batch(bw, args, device, max(3, args.steps // 4))
-    if pg:
-        t = torch.tensor([e2e_v], dtype=torch.float64)
-        pg.all_reduce(t)
-        e2e_v = float(t.item())
+    _, (e2e_v,) = aggregate(pg, 0.0, [e2e_v])
     single = None if args.no_single else single_tree(args, device, rank)
     nstate = None if args.no_single else {"aa_20_states": nstate_forms("aa", device),
                                           "codon_61_states": nstate_forms("codon", device)}
