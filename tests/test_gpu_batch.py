@@ -6,6 +6,9 @@ three branches at the connector nd are optimised in GARLI's order nd->left, nd,
 nd->right (optimization.cpp:882-884).  The oracle does exactly that on the
 candidate tree with GARLI's CPU code path.
 
+Both GTR+G4 and GTR+I+G4 (the +I term enters every site likelihood of the
+constant patterns, scaled by the pattern's scalers).
+
 Tolerances:
   * plain FP64 per-tree path: rescore lnL to 1e-8 relative of the oracle;
     optimised lengths to 1e-6 relative, optimised lnL to 1e-8 relative;
@@ -23,11 +26,12 @@ from oracle import oracle as orc
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def case():
+@pytest.fixture(scope="module", params=["gtr_g4", "gtr_i_g4"])
+def case(request):
     if engine.lib().gb_get_device_count() < 1:
         pytest.fail("no CUDA device visible to the engine")
-    w = synth.make_dna(24, 1500, seed=41)
+    pinv = (0.05, 0.3) if request.param == "gtr_i_g4" else None
+    w = synth.make_dna(24, 1500, seed=41, pinv_range=pinv)
     c3s, dls, conn = synth.ga_candidates(w.child3, w.dlen, 12, seed=42, radius_range=(1, 6))
     ref = []
     for i in range(len(conn)):
