@@ -358,7 +358,7 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
                 void *f = tc_func(I->S, I->R, &tsm);
                 double corr = I->tc_corr;
                 void *args[] = {&v, &L, (void *)&first, &corr};
-                GB_CUDA(cudaLaunchKernel(f, dim3(nt, L.n), dim3(kTcM), args, tsm, I->stream));
+                GB_CUDA(cudaLaunchKernel(f, dim3(nt, L.n), dim3(kTcThreads), args, tsm, I->stream));
             }
         }
         int rc = check_launch(I);
@@ -1213,7 +1213,7 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                         size_t tsm = 0;
                         void *f = tc_func(I->S, I->R, &tsm);
                         void *args[] = {&v, &L, &first, &I->tc_corr};
-                        B.block = dim3(kTcM);
+                        B.block = dim3(kTcThreads);
                         rc = B.add(B.g, &prev, f, dim3(nt, L.n), tsm, args);
                         B.block = dim3(kThreads);
                     }

@@ -35,7 +35,8 @@ enum : int { kStatusTcTimeout = 8 };
 // 20- and 61-state test and benchmark alignments (0 ulp: -4e-8 relative lnL;
 // no correction of the accumulated form: -1.2e-7).
 constexpr double kTcCorrUlps = 0.66;
-constexpr int kTcM = 128;  // patterns per CTA (UMMA M)
+constexpr int kTcM = 128;      // patterns per CTA (UMMA M)
+constexpr int kTcThreads = 256;  // two warpgroups: both stage; each reads back half of the TMEM columns
 
 template <int S>
 struct TcShape {
@@ -110,46 +111,65 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
 }
 
 // Stage rows [p0, p0 + 128) of one child (CLA or tip) for category r as hi/lo
-// tf32 operands.
+// tf32 operands, four K-consecutive elements (one 16-byte core-matrix row
+// segment) per step; the global loads are float4 when rows are 16-byte aligned.
 template <int S, int R>
 __device__ __forceinline__ void tc_stage_a(const View &v, int child, bool tip, int p0, int r, unsigned char *hi,
                                            unsigned char *lo) {
-    constexpr int KP = TcShape<S>::KP;
+    constexpr int KP = TcShape<S>::KP, KQ = KP / 4;
+    constexpr bool VEC = (R * S) % 4 == 0 && S % 4 == 0;
     const float *src = tip ? nullptr : cla_ptr<float>(v, child, p0, R * S);
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < kTcM * KP; idx += blockDim.x) {
-        const int m = idx / KP, k = idx % KP;
+#pragma unroll 2
+    for (int idx = threadIdx.x; idx < kTcM * KQ; idx += blockDim.x) {
+        const int m = idx / KQ, k0 = (idx % KQ) * 4;
         const int p = p0 + m;
-        float x = 0.f;
-        if (k < S && p < v.npat) {
+        float x[4] = {0.f, 0.f, 0.f, 0.f};
+        if (p < v.npat) {
             if (tip) {
                 const int code = v.tips[(long long)child * v.npat_pad + p];
-                x = (code >= S || code == k) ? 1.f : 0.f;
+#pragma unroll
+                for (int j = 0; j < 4; j++) x[j] = (k0 + j < S && (code >= S || code == k0 + j)) ? 1.f : 0.f;
+            } else if (VEC && k0 + 4 <= S) {
+                const float4 q = __ldg(reinterpret_cast<const float4 *>(src + (long long)m * R * S + r * S + k0));
+                x[0] = q.x;
+                x[1] = q.y;
+                x[2] = q.z;
+                x[3] = q.w;
             } else {
-                x = __ldg(src + (long long)m * R * S + r * S + k);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k0 + j < S) x[j] = __ldg(src + (long long)m * R * S + r * S + k0 + j);
             }
         }
-        const float h = to_tf32(x);
-        const float l = to_tf32(x - h);
-        const uint32_t off = kmaj_off(m, k, KP);
-        *reinterpret_cast<float *>(hi + off) = h;
-        *reinterpret_cast<float *>(lo + off) = l;
+        float h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            h[j] = to_tf32(x[j]);
+            l[j] = to_tf32(x[j] - h[j]);
+        }
+        const uint32_t off = kmaj_off(m, k0, KP);
+        *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
     }
 }
 
 // Stage P_r (rows = "from" states i as N, columns = "to" states j as K).
 template <int S, int R>
 __device__ __forceinline__ void tc_stage_b(const View &v, int mat, int r, unsigned char *hi, unsigned char *lo) {
-    constexpr int KP = TcShape<S>::KP, NP = TcShape<S>::NP;
+    constexpr int KP = TcShape<S>::KP, NP = TcShape<S>::NP, KQ = KP / 4;
     const double *P = v.mats + (long long)mat * v.mat_stride + (long long)r * S * S;
-    for (int idx = threadIdx.x; idx < NP * KP; idx += blockDim.x) {
-        const int n = idx / KP, k = idx % KP;
-        const float x = (n < S && k < S) ? (float)__ldg(P + n * S + k) : 0.f;
-        const float h = to_tf32(x);
-        const float l = to_tf32(x - h);
-        const uint32_t off = kmaj_off(n, k, KP);
-        *reinterpret_cast<float *>(hi + off) = h;
-        *reinterpret_cast<float *>(lo + off) = l;
+    for (int idx = threadIdx.x; idx < NP * KQ; idx += blockDim.x) {
+        const int n = idx / KQ, k0 = (idx % KQ) * 4;
+        float h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float x = (n < S && k0 + j < S) ? (float)__ldg(P + n * S + k0 + j) : 0.f;
+            h[j] = to_tf32(x);
+            l[j] = to_tf32(x - h[j]);
+        }
+        const uint32_t off = kmaj_off(n, k0, KP);
+        *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
     }
 }
 
@@ -183,7 +203,7 @@ __device__ __forceinline__ double ulp_f(float f) {
 // A round = one child, RG categories, one 32-state half: stage, issue, wait,
 // read back.
 template <int S, int R>
-__global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int first_tile, double corr_ulps) {
+__global__ void __launch_bounds__(kTcThreads, 2) k_cla_tc(View v, LevelOps ops, int first_tile, double corr_ulps) {
     using SM = TcSmem<S, R>;
     constexpr int KP = SM::KP, KB = SM::KB, NH = SM::NH, RG = SM::RG;
     constexpr int GB = 2 * SM::A_BYTES + 2 * SM::B_BYTES;  // staging bytes of one category
@@ -194,7 +214,8 @@ __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int fi
     const DevOp op = ops.op[blockIdx.y];
     const int p0 = (first_tile + blockIdx.x) * kTcM;
     const int warp = threadIdx.x >> 5;
-    const int m = threadIdx.x;  // epilogue row (TMEM lane)
+    const int wg = threadIdx.x >> 7;  // warpgroup: which 8-column chunks it reads back
+    const int m = threadIdx.x & 127;  // epilogue row (TMEM lane; warp w reads lanes 32 (w % 4) ..)
     const int p = p0 + m;
     const uint32_t mbar = smem_u32(&s_mbar);
     if (warp == 0) {
@@ -210,7 +231,7 @@ __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int fi
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = s_taddr;
-    const uint32_t trow = taddr + ((uint32_t)(warp * 32) << 16);
+    const uint32_t trow = taddr + ((uint32_t)((warp & 3) * 32) << 16);
     constexpr uint32_t idesc = tc_idesc(32);
     const uint32_t sbo = KP * 32, lbo = 128;
     bool ok = true;
@@ -262,7 +283,7 @@ __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int fi
                 for (int g = 0; g < ng; g++) {
                     const uint32_t rbase = trow + (uint32_t)(g * SM::RCOLS);
                     const int r = r0 + g;
-                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                    for (int c8 = wg * 8; c8 < 32; c8 += 16) {
                         uint32_t t[KB + 1][8];
 #pragma unroll
                         for (int kb = 0; kb <= KB; kb++) tc_ld8_nw(rbase + kb * 32 + c8, t[kb]);
@@ -292,21 +313,32 @@ __global__ void __launch_bounds__(kTcM, 1) k_cla_tc(View v, LevelOps ops, int fi
     }
     if (!ok) {
         if (threadIdx.x == 0) atomicOr(v.status, kStatusTcTimeout);
-    } else if (p < v.npat) {
+    } else {
+        // row m: each warpgroup takes half of the R*S entries; the row max is combined in shared
+        // memory (the staging area, free once the last products are read back)
+        double(*s_mx)[kTcM] = reinterpret_cast<double(*)[kTcM]>(tc_smem);
         const double *row = prod + (long long)m * SM::RSP;
+        const int k0 = wg ? (R * S) / 2 : 0, k1 = wg ? R * S : (R * S) / 2;
         double mx = 0.0;
-        for (int k = 0; k < R * S; k++) mx = fmax(mx, row[k]);
-        int e = 0;
-        if (mx > 0.0) e = max(-1000, min(1000, ilogb(mx)));
-        const double sc = pow2d(-e);
-        float *dst = cla_ptr<float>(v, op.dest, p, R * S);
-        for (int k = 0; k < R * S; k++)
-            dst[k] = round_stochastic_exact(row[k] * sc,
-                                            (unsigned int)(reinterpret_cast<unsigned long long>(dst + k) >> 2));
-        int ms = 0;
-        if (op.kind != kTipTip) ms += v.scalers[(long long)op.c1 * v.npat_pad + p];
-        if (op.kind == kIntInt) ms += v.scalers[(long long)op.c2 * v.npat_pad + p];
-        v.scalers[(long long)op.dest * v.npat_pad + p] = ms - e;
+        for (int k = k0; k < k1; k++) mx = fmax(mx, row[k]);
+        s_mx[wg][m] = mx;
+        __syncthreads();
+        mx = fmax(s_mx[0][m], s_mx[1][m]);
+        if (p < v.npat) {
+            int e = 0;
+            if (mx > 0.0) e = max(-1000, min(1000, ilogb(mx)));
+            const double sc = pow2d(-e);
+            float *dst = cla_ptr<float>(v, op.dest, p, R * S);
+            for (int k = k0; k < k1; k++)
+                dst[k] = round_stochastic_exact(row[k] * sc,
+                                                (unsigned int)(reinterpret_cast<unsigned long long>(dst + k) >> 2));
+            if (wg == 0) {
+                int ms = 0;
+                if (op.kind != kTipTip) ms += v.scalers[(long long)op.c1 * v.npat_pad + p];
+                if (op.kind == kIntInt) ms += v.scalers[(long long)op.c2 * v.npat_pad + p];
+                v.scalers[(long long)op.dest * v.npat_pad + p] = ms - e;
+            }
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
