@@ -20,6 +20,7 @@
 #include "gb_batch_mixed.cuh"
 #include "gb_common.cuh"
 #include "gb_dna.cuh"
+#include "gb_eigen.cuh"
 #include "gb_graph.cuh"
 #include "gb_newton_dna.cuh"
 #include "gb_nstate.cuh"
@@ -277,6 +278,8 @@ static void *tc_func(int S, int R, size_t *smem) {
 
 static int set_smem_attrs() {
     const int big = 200 * 1024;
+    GB_CUDA(cudaFuncSetAttribute(k_eigen_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)eigen_smem_bytes(61)));
     for (int S : {20, 61})
         for (int R = 1; R <= 8; R++) {
             size_t sm = 0;
@@ -1974,6 +1977,69 @@ int gb_set_batch_tuning(int instance, int tilesPerItem, int chunksPerItem) {
     I->batch_tiles = tilesPerItem;
     I->batch_chunks = chunksPerItem;
     I->bgraph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_set_eigen_from_rate_matrices(int instance, int count, const int *eigenIndices, const double *Q,
+                                    const double *pi, const double *blenMults, int *sweepsOut) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (count < 1 || !eigenIndices || !Q || !pi || !blenMults) return GB_ERROR_OUT_OF_RANGE;
+    const int S = I->S;
+    for (int c = 0; c < count; c++) {
+        if (eigenIndices[c] < 0 || eigenIndices[c] >= I->neigen) return GB_ERROR_OUT_OF_RANGE;
+        for (int i = 0; i < S; i++)
+            if (!(pi[c * S + i] > 0.0)) return GB_ERROR_OUT_OF_RANGE;  // D^1/2 needs positive frequencies
+    }
+    cudaSetDevice(I->device);
+    double *dQ = nullptr, *dpi = nullptr;
+    EigenJob *djobs = nullptr;
+    int *dsw = nullptr;
+    auto release = [&]() {
+        cudaFree(dQ);
+        cudaFree(dpi);
+        cudaFree(djobs);
+        cudaFree(dsw);
+    };
+    if (cudaMalloc(&dQ, (size_t)count * S * S * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dpi, (size_t)count * S * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&djobs, (size_t)count * sizeof(EigenJob)) != cudaSuccess ||
+        cudaMalloc(&dsw, (size_t)count * sizeof(int)) != cudaSuccess) {
+        release();
+        g_last_error = "gb_set_eigen_from_rate_matrices: cudaMalloc failed";
+        return GB_ERROR_OUT_OF_MEMORY;
+    }
+    std::vector<EigenJob> jobs(count);
+    for (int c = 0; c < count; c++) {
+        jobs[c].Q = dQ + (size_t)c * S * S;
+        jobs[c].pi = dpi + (size_t)c * S;
+        jobs[c].blen_mult = blenMults[c];
+        jobs[c].out = I->d_eigen + (size_t)eigenIndices[c] * I->eig_stride();
+        jobs[c].sweeps = dsw + c;
+    }
+    int rc = GB_SUCCESS;
+    if (cudaMemcpyAsync(dQ, Q, (size_t)count * S * S * sizeof(double), cudaMemcpyHostToDevice, I->stream) ||
+        cudaMemcpyAsync(dpi, pi, (size_t)count * S * sizeof(double), cudaMemcpyHostToDevice, I->stream) ||
+        cudaMemcpyAsync(djobs, jobs.data(), (size_t)count * sizeof(EigenJob), cudaMemcpyHostToDevice, I->stream))
+        rc = GB_ERROR_GENERAL;
+    if (!rc) {
+        k_eigen_jacobi<<<count, 256, eigen_smem_bytes(S), I->stream>>>(djobs, S);
+        rc = check_launch(I);
+    }
+    std::vector<int> sw(count, 0);
+    if (!rc && cudaMemcpyAsync(sw.data(), dsw, (size_t)count * sizeof(int), cudaMemcpyDeviceToHost, I->stream))
+        rc = GB_ERROR_GENERAL;
+    if (cudaStreamSynchronize(I->stream) != cudaSuccess) rc = GB_ERROR_GENERAL;
+    release();
+    if (rc) return rc;
+    if (sweepsOut)
+        for (int c = 0; c < count; c++) sweepsOut[c] = sw[c];
+    for (int c = 0; c < count; c++)
+        if (sw[c] >= kJacobiMaxSweeps) {
+            g_last_error = "gb_set_eigen_from_rate_matrices: Jacobi iteration did not converge";
+            return GB_ERROR_FLOATING_POINT;
+        }
+    I->version++;
     return GB_SUCCESS;
 }
 

@@ -112,6 +112,7 @@ SIGNATURES = {
     "gb_set_tensor_cores": (C.c_int, [C.c_int, C.c_int]),
     "gb_set_tensor_core_correction": (C.c_int, [C.c_int, C.c_double]),
     "gb_set_buffer_precision": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "gb_set_eigen_from_rate_matrices": (C.c_int, [C.c_int, C.c_int, _I, _D, _D, _D, _I]),
     "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),
     "gbp_destroy": (C.c_int, [C.c_int]),
     "gbp_invalidate": (C.c_int, [C.c_int]),
@@ -360,6 +361,17 @@ class Instance:
 
     def synchronize(self):
         _chk(lib().gb_synchronize(self.h), "gb_synchronize")
+
+    def set_eigen_from_q(self, eigen_indices, Qs, pis, blen_mults):
+        """Eigensystems of rate matrices computed on the device (one CTA per model);
+        returns the Jacobi sweeps each took."""
+        idx = _i32(eigen_indices)
+        n = len(idx)
+        sw = np.zeros(n, dtype=np.int32)
+        _chk(lib().gb_set_eigen_from_rate_matrices(self.h, n, _p(idx, C.c_int), _p(_f64(Qs), C.c_double),
+                                                   _p(_f64(pis), C.c_double), _p(_f64(blen_mults), C.c_double),
+                                                   _p(sw, C.c_int)), "gb_set_eigen_from_rate_matrices")
+        return sw
 
     def set_tensor_cores(self, on: bool):
         _chk(lib().gb_set_tensor_cores(self.h, int(on)), "gb_set_tensor_cores")

@@ -119,6 +119,15 @@ int gb_set_eigen_decomposition(int instance, int eigenIndex, const double *eigen
                                const double *inverseEigenVectors, const double *eigenValues);
 
 /* ---- operations ---- */
+/* Model::CalcEigenStuff (model.cpp:827-856) on the device, FP64, one CTA per
+ * model: for each c, the eigensystem of the reversible rate matrix
+ * Q[c*S*S ...] (row-major) with stationary frequencies pi[c*S ...] (all > 0)
+ * into eigen slot eigenIndices[c], eigenvalues multiplied by blenMults[c]
+ * (model.cpp:845).  Symmetrised by diag(pi)^1/2 and diagonalised by cyclic
+ * Jacobi; sweepsOut[c] (optional) = Jacobi sweeps used.  For the many models
+ * of a model-parameter optimisation at once (optimization.cpp:332-776). */
+int gb_set_eigen_from_rate_matrices(int instance, int count, const int *eigenIndices, const double *Q,
+                                    const double *pi, const double *blenMults, int *sweepsOut);
 /* beagleUpdateTransitionMatrices (subsetcalculationmanager.cpp:232): P(t) and,
  * if requested, dP/dt and d2P/dt2 in FP64 on the device (model.cpp:1271,:1469) */
 int gb_update_transition_matrices(int instance, const gb_transmat_operation *ops, int count);
