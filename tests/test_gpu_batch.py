@@ -88,3 +88,18 @@ def test_batched_precision_form_matches_oracle_and_repeats(case):
     ncand = len(case[3])
     per = (cnt["cla_ops"] - 3 * ncand) / ncand
     assert 1 <= per <= 60
+
+
+def test_population_switches_between_batched_and_per_tree_modes(case):
+    """One precision-form population: batched (parent tree in FP64 buffers), then
+    per-tree (parent rebuilt in ordinary buffers), then batched again."""
+    w, c3s, dls, conn, ref = case
+    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), mixed=True)
+    tol = 1e-4 * max(1.0, w.data.npat / 2000)
+    runs = [pop.score(c3s, dls, conn, 0.01, sequential=s)[0] for s in (False, True, False)]
+    for out in runs:
+        for i, (l0, lf, _) in enumerate(ref):
+            assert abs(out[i, 0] - l0) <= tol and abs(out[i, 1] - lf) <= tol
+    assert np.array_equal(runs[0], runs[2])
+    pop.close()
+    inst.close()
