@@ -79,3 +79,28 @@ def test_argument_checks_without_device():
     assert L.gb_create_instance(11, 27, 4, 100, 1, 20, 9, 0, 1, C.byref(det)) == -5
     assert L.gb_finalize_instance(12345) == -4
     assert L.gbt_score(999, 0, (C.c_double * 3)()) == -4
+
+
+def test_new_entry_points_reject_bad_handles_and_sizes_without_device():
+    """Batched pass, population layer, device eigensolver, tensor-core and FP64
+    buffer switches, and the allocation-free edge: invalid handles and sizes are
+    rejected before any device work."""
+    L = engine.lib()
+    d3 = (C.c_double * 12)()
+    i4 = (C.c_int * 4)()
+    assert L.gb_batch_newton(4321, None, 0, None, 0, None, 1, 3, 16, 0.01, 1e-8, 100.0, d3) == -4
+    assert L.gb_set_batch_tuning(4321, 1, 1) == -4
+    assert L.gb_get_batch_tuning(4321, i4) == -4
+    assert L.gb_set_tensor_cores(4321, 1) == -4
+    assert L.gb_set_tensor_core_correction(4321, 0.5) == -4
+    assert L.gb_set_buffer_precision(4321, 10, 1) == -4
+    assert L.gb_set_eigen_from_rate_matrices(4321, 1, i4, d3, d3, d3, None) == -4
+    assert L.gbp_score_candidates(4321, 1, i4, d3, i4, 0.01, 0, d3, d3) == -4
+    assert L.gbp_get_counters(4321, (C.c_longlong * 6)()) == -4
+    assert L.gbp_destroy(4321) == -4
+    assert L.gbp_create(4321, 8, i4, d3, 10) == -4
+    # the allocation-free edge checks its pattern limit first
+    assert L.gb_edge_loglik_static(0, 4, (1 << 22) + 1, None, None, None, None, None, None, None, None, None, None,
+                                   0.0, 0, 1, None, None) == -5
+    assert L.gb_edge_loglik_static(0, 9, 100, None, None, None, None, None, None, None, None, None, None, 0.0, 0, 1,
+                                   None, None) == -5
