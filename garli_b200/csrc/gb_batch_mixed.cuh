@@ -5,7 +5,7 @@
 //             blocks in padded shared memory, FP64 fused arithmetic, the
 //             pattern's power-of-two normalisation by a shuffle max, FP32
 //             stores with unbiased stochastic rounding (exact, no division);
-//             the child loads of kU tiles are issued before any arithmetic.
+//             both children's loads are issued before any arithmetic.
 //   kBCoef  : for every candidate's step, the spectral coefficients of the
 //             branch it optimises.  With P_r(t) = U diag(exp(s_rk t)) U^-1,
 //             s_rk = lambda_k rate_r / (1 - pinv),
@@ -14,11 +14,15 @@
 //             where W = (P_o1 V_o1) o (P_o2 V_o2) is the partial on the
 //             connector's side, formed in FP64 registers and never stored,
 //             and V the CLA (or tip) across the branch.  One lane per
-//             (pattern, category), loads first as in kBLevel.  A is FP64,
-//             laid out [slot][r*4+k][pattern]; the site's scale exponent is
-//             m_o1 + m_o2 + m_V.
+//             (pattern, category), loads first as in kBLevel.  A is FP64.
+//             A reversible rate matrix's rows sum to zero, so one eigenvalue
+//             lambda_k0 is zero (to rounding) and exp(s_rk0 t) = 1 for every
+//             category and length: its R coefficients are stored as one sum,
+//             1 + 3R per pattern, laid out [slot][q][pattern] with q = 0 the
+//             stationary sum and q = 1 + 3r + j the j-th other eigenvalue of
+//             category r; the site's scale exponent is m_o1 + m_o2 + m_V.
 //   kBNewton: Newton-Raphson in lockstep; an iteration reads only A:
-//             L = sum A e, dL/dt = sum A s e, d2L/dt2 = sum A s^2 e with the
+//             L = A_0 + sum A e, dL/dt = sum A s e, d2L/dt2 = sum A s^2 e with the
 //             per-candidate tables e, s e, s^2 e recomputed in FP64 after
 //             every step.  A chunk = 256 patterns summed by one warp (8 per
 //             lane, then a shuffle tree) -- no block barrier; the candidate's
@@ -51,9 +55,9 @@ struct MixedArgs {
     double *lengths;
     const double *eig;    // lambda (scaled), U, U^-1
     const double *rates;
-    double *coef;         // max_entries x 16R... [slot][R*4][npat_pad]
+    double *coef;         // [slot][1 + 3R][npat_pad]
     int *cscale;          // max_entries x npat_pad
-    double *etab;         // max_entries x 3 x R*4
+    double *etab;         // max_entries x 3 x (1 + 3R)
     double *chunk_sums;   // max_entries x nchunks x 3
     int *active;
     int *nactive;
@@ -155,9 +159,9 @@ __device__ __forceinline__ void slice_load(const View &v, int b, bool wide, int 
 
 // CLA update of tiles [t0, t1) of one op; lane = category r of pattern
 // tile * PPB + threadIdx.x / G; PL, PR = the category's P blocks in shared
-// memory.  Tiles run in groups of kU with every child load of the group
-// issued before any arithmetic (memory-level parallelism).
-constexpr int kU = 2;
+// memory.  Both children's loads of a tile are issued before its arithmetic;
+// one tile at a time: holding a second tile's loads in flight spilled
+// registers in the batched kernel and measured slower.
 template <int R>
 __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, const double *PL, const double *PR,
                                             int t0, int t1, int r, bool lane_ok) {
@@ -165,46 +169,35 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
     constexpr int PPB = kThreads / G;
     const int pl = threadIdx.x / G;
     const bool w1 = op.wide & kWideC1, w2 = op.wide & kWideC2, wd = op.wide & kWideDest;
-    for (int tile = t0; tile < t1; tile += kU) {
-        double A[kU][4], B[kU][4];
-        int M[kU];
-        unsigned char T1[kU], T2[kU];
-#pragma unroll
-        for (int u = 0; u < kU; u++) {
-            const int p = (tile + u) * PPB + pl;
-            const bool act = lane_ok && tile + u < t1 && p < v.npat;
-            M[u] = 0;
-            T1[u] = T2[u] = 15;
-            if (!act) continue;
+    for (int tile = t0; tile < t1; tile++) {
+        const int p = tile * PPB + pl;
+        const bool act = lane_ok && p < v.npat;
+        double a[4], b[4], d[4] = {0, 0, 0, 0};
+        int m = 0;
+        unsigned char c1 = 15, c2 = 15;
+        if (act) {
             if (op.kind == kTipTip) {
-                T1[u] = v.tips[(long long)op.c1 * v.npat_pad + p];
-                T2[u] = v.tips[(long long)op.c2 * v.npat_pad + p];
-                continue;
-            }
-            slice_load<R>(v, op.c1, w1, p, r, A[u]);
-            M[u] = __ldcg(v.scalers + (long long)op.c1 * v.npat_pad + p);
-            if (op.kind == kIntInt) {
-                slice_load<R>(v, op.c2, w2, p, r, B[u]);
-                M[u] += __ldcg(v.scalers + (long long)op.c2 * v.npat_pad + p);
+                c1 = v.tips[(long long)op.c1 * v.npat_pad + p];
+                c2 = v.tips[(long long)op.c2 * v.npat_pad + p];
             } else {
-                T2[u] = v.tips[(long long)op.c2 * v.npat_pad + p];
+                slice_load<R>(v, op.c1, w1, p, r, a);
+                m = __ldcg(v.scalers + (long long)op.c1 * v.npat_pad + p);
+                if (op.kind == kIntInt) {
+                    slice_load<R>(v, op.c2, w2, p, r, b);
+                    m += __ldcg(v.scalers + (long long)op.c2 * v.npat_pad + p);
+                } else {
+                    c2 = v.tips[(long long)op.c2 * v.npat_pad + p];
+                }
             }
-        }
+            double x[4], y[4];
+            if (op.kind == kTipTip) pvec_tip(PL, c1, x);
+            else pvec(PL, a, x);
+            if (op.kind == kIntInt) pvec(PR, b, y);
+            else pvec_tip(PR, c2, y);
 #pragma unroll
-        for (int u = 0; u < kU; u++) {
-            const int p = (tile + u) * PPB + pl;
-            const bool act = lane_ok && tile + u < t1 && p < v.npat;
-            double d[4] = {0, 0, 0, 0}, x[4], y[4];
-            if (act) {
-                if (op.kind == kTipTip) pvec_tip(PL, T1[u], x);
-                else pvec(PL, A[u], x);
-                if (op.kind == kIntInt) pvec(PR, B[u], y);
-                else pvec_tip(PR, T2[u], y);
-#pragma unroll
-                for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
-            }
-            cla_finish_m<R>(v, op.dest, wd, p, r, act, d, M[u]);
+            for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
         }
+        cla_finish_m<R>(v, op.dest, wd, p, r, act, d, m);
     }
 }
 
@@ -245,72 +238,116 @@ __device__ __forceinline__ void side_vec(const double c[4], int code, int tip, c
     }
 }
 
-// Coefficients A[r][k], k = 0..3, of category r at pattern p from the three
-// side vectors; stored to the entry's slot.
+// coefficients per pattern: the stationary sum and 3 per category
 template <int R>
-__device__ __forceinline__ void coef_store(const View &v, const MixedArgs &A, int slot, int p, int r, const double x[4],
-                                           const double y[4], const double z[4], int scale, const double *sU,
-                                           const double *sUi) {
-    double w[4];
+struct Coefs {
+    static constexpr int N = 1 + 3 * R;
+};
+
+// the stationary eigenvalue: the one of least magnitude
+__device__ __forceinline__ int stationary_index(const double *eig) {
+    int k0 = 0;
+    double m = fabs(__ldg(eig));
+#pragma unroll
+    for (int k = 1; k < 4; k++) {
+        const double a = fabs(__ldg(eig + k));
+        if (a < m) {
+            m = a;
+            k0 = k;
+        }
+    }
+    return k0;
+}
+
+// Coefficients of category r at pattern p from the three side vectors, stored
+// to the entry's slot: the 3 non-stationary ones of the lane's category, and
+// the stationary one summed over the pattern's G lanes (lane_ok false: a
+// zero share).  All G lanes of the pattern must call this together.
+template <int R>
+__device__ __forceinline__ void coef_store(const View &v, const MixedArgs &A, int slot, int p, int r, bool act,
+                                           const double x[4], const double y[4], const double z[4], int scale,
+                                           const double *sU, const double *sUi, int k0) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int NC = Coefs<R>::N;
+    double w[4], c[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) w[i] = x[i] * y[i] * v.freqs[i];
-    const double rp = v.rate_probs[r];
+    const double rp = act ? v.rate_probs[r] : 0.0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const double a_k = fma(w[3], sU[12 + k], fma(w[2], sU[8 + k], fma(w[1], sU[4 + k], w[0] * sU[k])));
         const double b_k = fma(sUi[k * 4 + 3], z[3], fma(sUi[k * 4 + 2], z[2], fma(sUi[k * 4 + 1], z[1], sUi[k * 4] * z[0])));
-        A.coef[((long long)slot * R * 4 + r * 4 + k) * v.npat_pad + p] = rp * a_k * b_k;
+        c[k] = act ? rp * a_k * b_k : 0.0;
     }
-    if (r == 0) A.cscale[(long long)slot * v.npat_pad + p] = scale;
+    double c0 = c[0];
+#pragma unroll
+    for (int k = 1; k < 4; k++)
+        if (k == k0) c0 = c[k];
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+    if (!act) return;
+    double *out = A.coef + (long long)slot * NC * v.npat_pad + p;
+    int j = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (k != k0) out[(long long)(1 + 3 * r + j++) * v.npat_pad] = c[k];
+    if (r == 0) {
+        out[0] = c0;
+        A.cscale[(long long)slot * v.npat_pad + p] = scale;
+    }
 }
 
 // Coefficient pass of tiles [t0, t1) of one entry; lane = category r of
 // pattern tile * PPB + threadIdx.x / G.  P1, P2 = the sides' P blocks of
-// category r (null: no matrix), sU / sUi = U and U^-1 in shared memory.
+// category r (null: no matrix), sU / sUi = U and U^-1 in shared memory.  One
+// tile per load batch: three sides' slices per lane already fill the registers.
 template <int R>
 __device__ __forceinline__ void coef_tiles_m(const View &v, const MixedArgs &A, const MEntry &en, const double *P1,
                                              const double *P2, const double *sU, const double *sUi, int slot, int t0,
-                                             int t1, int r, bool lane_ok) {
+                                             int t1, int r, bool lane_ok, int k0) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     const int pl = threadIdx.x / G;
     const bool w1 = en.wide & 1, w2 = en.wide & 2, wk = en.wide & 4;
-    for (int tile = t0; tile < t1; tile += kU) {
-        SideRaw S1[kU], S2[kU], SK[kU];
-#pragma unroll
-        for (int u = 0; u < kU; u++) {
-            const int p = (tile + u) * PPB + pl;
-            const bool act = lane_ok && tile + u < t1 && p < v.npat;
-            side_load<R>(v, act ? en.b1 : -1, en.t1, w1, p, r, S1[u]);
-            side_load<R>(v, act ? en.b2 : -1, en.t2, w2, p, r, S2[u]);
-            side_load<R>(v, act ? en.bk : -1, en.tk, wk, p, r, SK[u]);
+    for (int tile = t0; tile < t1; tile++) {
+        const int p = tile * PPB + pl;
+        const bool act = lane_ok && p < v.npat;
+        SideRaw S1, S2, SK;
+        side_load<R>(v, act ? en.b1 : -1, en.t1, w1, p, r, S1);
+        side_load<R>(v, act ? en.b2 : -1, en.t2, w2, p, r, S2);
+        side_load<R>(v, act ? en.bk : -1, en.tk, wk, p, r, SK);
+        double x[4] = {0, 0, 0, 0}, y[4] = {1, 1, 1, 1}, z[4] = {0, 0, 0, 0};
+        if (act) {
+            side_vec(S1.c, S1.code, en.t1, P1, x);
+            if (en.b2 >= 0) side_vec(S2.c, S2.code, en.t2, P2, y);
+            side_vec(SK.c, SK.code, en.tk, nullptr, z);
         }
-#pragma unroll
-        for (int u = 0; u < kU; u++) {
-            const int p = (tile + u) * PPB + pl;
-            if (!(lane_ok && tile + u < t1 && p < v.npat)) continue;
-            double x[4], y[4] = {1, 1, 1, 1}, z[4];
-            side_vec(S1[u].c, S1[u].code, en.t1, P1, x);
-            if (en.b2 >= 0) side_vec(S2[u].c, S2[u].code, en.t2, P2, y);
-            side_vec(SK[u].c, SK[u].code, en.tk, nullptr, z);
-            coef_store<R>(v, A, slot, p, r, x, y, z, S1[u].scale + S2[u].scale + SK[u].scale, sU, sUi);
-        }
+        coef_store<R>(v, A, slot, p, r, act, x, y, z, S1.scale + S2.scale + SK.scale, sU, sUi, k0);
     }
 }
 
-// e, s e, s^2 e of all (r, k) at length t, by one warp, into etab[3][R*4]
+// e, s e, s^2 e of every stored coefficient at length t, by one warp, into
+// etab[3][1 + 3R]; the stationary one is exactly (1, 0, 0)
 template <int R>
 __device__ __forceinline__ void etab_warp(const double *eig, const double *rates, double pinv, int has_pinv, double t,
                                           double *etab) {
+    constexpr int NC = Coefs<R>::N;
     const int lane = threadIdx.x & 31;
-    for (int idx = lane; idx < R * 4; idx += 32) {
-        const int r = idx / 4, k = idx % 4;
-        double s = __ldcg(eig + k) * __ldcg(rates + r);
-        if (has_pinv) s = s / (1.0 - pinv);
-        const double e = exp(s * t);
-        etab[idx] = e;
-        etab[R * 4 + idx] = s * e;
-        etab[2 * R * 4 + idx] = s * s * e;
+    const int k0 = stationary_index(eig);
+    for (int q = lane; q < NC; q += 32) {
+        double e = 1.0, se = 0.0, s2e = 0.0;
+        if (q > 0) {
+            const int r = (q - 1) / 3, j = (q - 1) % 3;
+            const int k = j < k0 ? j : j + 1;
+            double s = __ldcg(eig + k) * __ldcg(rates + r);
+            if (has_pinv) s = s / (1.0 - pinv);
+            e = exp(s * t);
+            se = s * e;
+            s2e = s * se;
+        }
+        etab[q] = e;
+        etab[NC + q] = se;
+        etab[2 * NC + q] = s2e;
     }
 }
 
@@ -319,20 +356,21 @@ template <int R>
 __device__ __forceinline__ void sweep_chunk(const View &v, const MixedArgs &A, int slot, const double *E, int c,
                                             double *sums) {
     const int lane = threadIdx.x & 31;
+    constexpr int NC = Coefs<R>::N;
     double aL = 0.0, a1 = 0.0, a2 = 0.0;
-    const double *cf = A.coef + (long long)slot * R * 4 * v.npat_pad;
+    const double *cf = A.coef + (long long)slot * NC * v.npat_pad;
     const int *cs = A.cscale + (long long)slot * v.npat_pad;
 #pragma unroll 2
     for (int j = 0; j < 8; j++) {
         const int p = c * 256 + j * 32 + lane;
         if (p >= v.npat) break;
-        double L = 0.0, D1 = 0.0, D2 = 0.0;
+        double L = __ldcg(cf + p), D1 = 0.0, D2 = 0.0;
 #pragma unroll
-        for (int q = 0; q < R * 4; q++) {
+        for (int q = 1; q < NC; q++) {
             const double a = __ldcg(cf + (long long)q * v.npat_pad + p);
             L = fma(a, E[q], L);
-            D1 = fma(a, E[R * 4 + q], D1);
-            D2 = fma(a, E[2 * R * 4 + q], D2);
+            D1 = fma(a, E[NC + q], D1);
+            D2 = fma(a, E[2 * NC + q], D2);
         }
         const int m = __ldcg(cs + p);
         const int cb = v.const_states[p];
@@ -367,11 +405,35 @@ __device__ __forceinline__ void sweep_chunk(const View &v, const MixedArgs &A, i
 // keeps the categories of a warp in different banks)
 constexpr int kPStride = 17;
 
+// A precision-form CLA level as a launch of its own (the per-tree path and the
+// graph-resident pass): the batched kernel's CLA code, blockIdx.y = the op, the
+// block's P blocks in shared memory, grid-stride over groups of kCla4mTiles tiles.
+constexpr int kCla4mTiles = 4;
+template <int R>
+__global__ void __launch_bounds__(kThreads, 2) k_cla4m(View v, LevelOps ops) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    __shared__ double sP[2][R][kPStride];
+    const DevOp op = ops.op[blockIdx.y];
+    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+        const int mi = q / (R * 16), rem = q % (R * 16);
+        sP[mi][rem / 16][rem % 16] = __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
+    }
+    __syncthreads();
+    const int cr = threadIdx.x % G;
+    const bool ok = cr < R;
+    const int crr = ok ? cr : 0;
+    const int ntiles = (v.npat + PPB - 1) / PPB;
+    for (int t0 = blockIdx.x * kCla4mTiles; t0 < ntiles; t0 += gridDim.x * kCla4mTiles)
+        cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ntiles, t0 + kCla4mTiles), crr, ok);
+}
+
 template <int R>
 __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;           // patterns per CLA tile
-    __shared__ double sE[8][3 * R * 4];  // one E table per warp
+    constexpr int NC = Coefs<R>::N;
+    __shared__ double sE[8][3 * NC];  // one E table per warp
     __shared__ double sP[2][R][kPStride];
     __shared__ double sUU[32];  // U, U^-1 of the model
     const int lane = threadIdx.x & 31;
@@ -429,6 +491,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
             const long long nitems = (long long)n * items_per_entry;
             int loaded = -1;
             MEntry en;
+            const int k0 = stationary_index(A.eig);
             for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
                 const int e = (int)(item / items_per_entry);
                 const int t0 = (int)(item % items_per_entry) * tpi;
@@ -445,7 +508,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
                     __syncthreads();
                 }
                 coef_tiles_m<R>(v, A, en, en.m1 >= 0 ? sP[0][crr] : nullptr, en.m2 >= 0 ? sP[1][crr] : nullptr, sUU,
-                                sUU + 16, e, t0, min(ctiles, t0 + tpi), crr, cla_ok);
+                                sUU + 16, e, t0, min(ctiles, t0 + tpi), crr, cla_ok, k0);
             }
             if (!grid_barrier(A.gs, v.status)) return;
             mark(kBtCmdDone, 0);
@@ -459,7 +522,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
                 nr_init(slots[e].st, t, A.prm.min_brlen, A.prm.max_brlen);
                 slots[e].evals = 0;
             }
-            etab_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t, A.etab + (long long)e * 3 * R * 4);
+            etab_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t, A.etab + (long long)e * 3 * NC);
             if (lane == 0) A.active[e] = e;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -484,7 +547,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
                 if (e != loaded) {
                     loaded = e;
                     __syncwarp();
-                    for (int q = lane; q < 3 * R * 4; q += 32) sE[warp][q] = __ldcg(A.etab + (long long)e * 3 * R * 4 + q);
+                    for (int q = lane; q < 3 * NC; q += 32) sE[warp][q] = __ldcg(A.etab + (long long)e * 3 * NC + q);
                     __syncwarp();
                 }
                 const int c1 = min(nchunks, c0 + cpi);
@@ -520,7 +583,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
                 if (newton) {
                     fin = __shfl_sync(0xffffffffu, fin, 0);
                     t = __shfl_sync(0xffffffffu, t, 0);
-                    etab_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t, A.etab + (long long)e * 3 * R * 4);
+                    etab_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t, A.etab + (long long)e * 3 * NC);
                     pmat4_warp<R>(A.eig, A.rates, v.pinv, v.has_pinv, t,
                                   const_cast<double *>(v.mats) + (long long)ents[e].mk * v.mat_stride);
                     if (!fin && lane == 0) {

@@ -207,20 +207,6 @@ static int upload_rescale_tables() {
 // ---------------------------------------------------------------------------
 // kernel dispatch
 // ---------------------------------------------------------------------------
-template <bool G>
-static void launch_cla4(int R, dim3 grid, cudaStream_t st, const View &v, const LevelOps &ops) {
-    switch (R) {
-        case 1: k_cla4<1, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 2: k_cla4<2, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 3: k_cla4<3, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 4: k_cla4<4, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 5: k_cla4<5, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 6: k_cla4<6, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        case 7: k_cla4<7, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-        default: k_cla4<8, G><<<grid, kThreads, 0, st>>>(v, ops); break;
-    }
-}
-
 template <bool G, bool D>
 static void launch_edge4(int R, int grid, cudaStream_t st, const View &v, int pb, int cb, int mat, int tip,
                          int ws) {
@@ -322,10 +308,13 @@ static void *pass4_func(int R, bool garli) {
 static dim3 cla4_grid(const Instance *I, int nops) {
     const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
     const int ppb = kThreads / G;
-    const int ntiles = (I->npat + ppb - 1) / ppb;
+    // the precision form's k_cla4m takes kCla4mTiles tiles per block step
+    const int ntiles = (I->npat + ppb - 1) / ppb, step = I->mixed ? kCla4mTiles : 1;
     const int want = (16 * I->nsm + nops - 1) / nops;
-    return dim3(std::max(1, std::min(ntiles, want)), nops);
+    return dim3(std::max(1, std::min((ntiles + step - 1) / step, want)), nops);
 }
+
+static void *cla4_func(int R, bool garli);
 
 static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleEvery) {
     View v = make_view(I);
@@ -342,8 +331,8 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
         }
         if (I->S == 4) {
             const dim3 grid = cla4_grid(I, L.n);
-            if (I->mixed) launch_cla4<false>(I->R, grid, I->stream, v, L);
-            else launch_cla4<true>(I->R, grid, I->stream, v, L);
+            void *args[] = {&v, &L};
+            GB_CUDA(cudaLaunchKernel(cla4_func(I->R, !I->mixed), grid, dim3(kThreads), args, 0, I->stream));
         } else {
             size_t smem;
             const int tp = ns_cla_tile(I, &smem);
@@ -1111,9 +1100,10 @@ static unsigned long long fnv(unsigned long long h, const void *p, size_t n) {
     return h;
 }
 
+// the plain form's k_cla4 (GARLI's rescaling) or the precision form's k_cla4m
 static void *cla4_func(int R, bool garli) {
 #define GB_CASE(r) \
-    case r: return garli ? (void *)k_cla4<r, true> : (void *)k_cla4<r, false>;
+    case r: return garli ? (void *)k_cla4<r, true> : (void *)k_cla4m<r>;
     switch (R) {
         GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
     }
@@ -1873,9 +1863,9 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
                                 I->d_mentries, I->d_coef, I->d_cscale, I->d_etab};
         if (I->mixed &&
             ((rc = grow_device(&I->d_mentries, &I->cap_mentries, nent)) ||
-             (rc = grow_device(&I->d_coef, &I->cap_coef, (size_t)nC * I->R * 4 * I->npat_pad)) ||
+             (rc = grow_device(&I->d_coef, &I->cap_coef, (size_t)nC * (1 + 3 * I->R) * I->npat_pad)) ||
              (rc = grow_device(&I->d_cscale, &I->cap_cscale, (size_t)nC * I->npat_pad)) ||
-             (rc = grow_device(&I->d_etab, &I->cap_etab, (size_t)nC * 3 * I->R * 4)))) {
+             (rc = grow_device(&I->d_etab, &I->cap_etab, (size_t)nC * 3 * (1 + 3 * I->R))))) {
             I->rank = rank_before;
             return rc;
         }

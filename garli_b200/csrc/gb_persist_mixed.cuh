@@ -8,7 +8,7 @@
 // arithmetic, not its decisions' structure:
 //   * CLA levels use the batched kernel's code (cla_tiles_m): one lane per
 //     (pattern, category), the op's P blocks in shared memory, FP64 fused
-//     arithmetic, loads of two tiles issued before any arithmetic,
+//     arithmetic, both children's loads issued before any arithmetic,
 //     division-free stochastic rounding of the FP32 stores;
 //   * the edge sweep loads the partial and child slices of all categories
 //     first and evaluates P, dP, d2P with fused FP64 multiply-adds.

@@ -143,7 +143,7 @@ struct Pop {
     std::vector<int> wide_bufs;    // buffers currently marked FP64
     long long c_ops = 0, c_updates = 0, c_evals = 0, c_base_ops = 0, c_edges = 0;
     double c_bytes = 0.0;
-    int npat = 0;
+    int npat = 0, ncat = 1;
 };
 
 std::mutex g_mu;
@@ -360,17 +360,23 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
 // evaluation pattern reads 128 + 4 + 4 + 4 B (coefficients, scale, count,
 // constant state).  See gbp_get_counters.
 double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps) {
+    // per pattern: a CLA slice is 4R FP32 values and a 4-byte scale exponent
+    // (FP64 values for the parent tree's wide buffers), a tip one byte; a
+    // step's coefficients are 1 + 3R doubles and a scale exponent; a sweep
+    // reads those and the pattern's count and constant-state word
+    const double cla = 16.0 * p.ncat + 4.0, wide = 32.0 * p.ncat + 4.0;
+    const double coef = 8.0 * (1 + 3 * p.ncat) + 4.0, sweep = coef + 8.0;
     auto side = [&](int b) {
         if (b < p.ntip) return 1.0;
-        return (p.base_mode == 1 && !p.wide_bufs.empty() && b < p.base_bufs) ? 132.0 : 68.0;
+        return (p.base_mode == 1 && !p.wide_bufs.empty() && b < p.base_bufs) ? wide : cla;
     };
     double per = 0.0;
-    for (const gb_cla_operation &o : P.ops) per += side(o.childClaIndex1) + side(o.childClaIndex2) + 68.0;
+    for (const gb_cla_operation &o : P.ops) per += side(o.childClaIndex1) + side(o.childClaIndex2) + cla;
     for (int i = 0; i < 3 * nC; i++) {
         const gb_cla_operation &o = P.step_ops[i];
-        per += 132.0 + side(o.childClaIndex1) + side(o.childClaIndex2) + side(P.steps[i].childIndex);
+        per += coef + side(o.childClaIndex1) + side(o.childClaIndex2) + side(P.steps[i].childIndex);
     }
-    per += 140.0 * (double)sweeps;
+    per += sweep * (double)sweeps;
     return per * (double)p.npat;
 }
 
@@ -451,6 +457,7 @@ int gbp_create(int instance, int ntax, const int *child3, const double *dlen, in
     p->ntip = shape[0];
     p->nbuf = shape[1];
     p->npat = shape[4];
+    p->ncat = shape[3];
     p->nmat = matrixCount;
     p->mat_len.assign(p->nmat, 0.0);
     std::lock_guard<std::mutex> lk(g_mu);

@@ -291,10 +291,11 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
 /* last call: [0] CLA updates (the per-step partials included), [1] pattern-updates,
  * [2] derivative evaluations, [4] edge evaluations (derivative evaluations + the
  * final scores), [5] algorithmic device-memory bytes of the precision form's
- * batched pass, per pattern at 4 categories: a CLA read 68 B (FP32 + scaler),
- * 132 B for an FP64 parent-tree CLA, 1 B for a tip; 68 B per CLA update
- * written; 132 B per coefficient pattern written; 140 B per edge-evaluation
- * pattern; [3] base-tree CLA updates since creation */
+ * batched pass, per pattern at R rate categories: a CLA read 16R + 4 B (FP32
+ * + scale exponent), 32R + 4 B for an FP64 parent-tree CLA, 1 B for a tip;
+ * 16R + 4 B per CLA update written; 8(1 + 3R) + 4 B per coefficient pattern
+ * written; 8(1 + 3R) + 12 B per edge-evaluation pattern (at R = 4: 68, 132,
+ * 108, 116); [3] base-tree CLA updates since creation */
 int gbp_get_counters(int pop, long long *out6);
 
 /* ---- edge evaluation without device allocation ----
