@@ -31,6 +31,7 @@
 // lnL, d1, d2 accumulate in FP64; the Newton step and P(t) are FP64.
 #pragma once
 #include "gb_batch.cuh"
+#include "gb_stage.cuh"
 
 namespace gb {
 
@@ -198,6 +199,123 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
             for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
         }
         cla_finish_m<R>(v, op.dest, wd, p, r, act, d, m);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Prefetched CLA tiles: every lane copies its own inputs of the tiles ahead
+// into its own shared-memory slots with asynchronous copies (cp.async, 16
+// bytes, through L2), kCpStages - 1 tiles ahead of the arithmetic, so a lane
+// keeps several tiles' loads in flight without holding them in registers and
+// without block barriers (a lane reads only what it copied).  Per lane and
+// stage: child 1's slice (32 B), child 2's slice (32 B), and two 16-byte
+// words holding the pattern's scale exponent or tip code (the aligned
+// 16-byte block that contains it).  Layout [stage][field][lane].
+constexpr int kCpStages = 3;
+constexpr int kCpLane = 96;  // bytes per lane and stage
+__host__ __device__ constexpr int cp_smem_bytes() { return kCpStages * kCpLane * kThreads; }
+
+struct CpSlots {
+    unsigned char *a, *b, *c, *d;  // this lane's slots of one stage
+};
+__device__ __forceinline__ CpSlots cp_slots(unsigned char *cps, int stage) {
+    unsigned char *s = cps + stage * kCpLane * kThreads;
+    const int t = threadIdx.x;
+    return {s + t * 32, s + 32 * kThreads + t * 32, s + 64 * kThreads + t * 16, s + 80 * kThreads + t * 16};
+}
+
+// the copies of tile `tile` for this lane (none past t1 or for an idle lane), one commit group
+template <int R>
+__device__ __forceinline__ void cp_issue(const View &v, const DevOp &op, int tile, int t1, int r, bool lane_ok,
+                                         unsigned char *cps, int stage) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    const int p = tile * PPB + threadIdx.x / G;
+    if (lane_ok && tile < t1 && p < v.npat) {
+        const CpSlots sl = cp_slots(cps, stage);
+        auto slice = [&](unsigned char *dst, int b, bool wide) {
+            if (wide || p < v.kpad) {
+                const double *src = (wide ? cla_ptr_wide(v, b, p, R * 4) : cla_ptr<double>(v, b, p, R * 4)) + r * 4;
+                cp16(smem_u32(dst), src);
+                cp16(smem_u32(dst + 16), src + 2);
+            } else {
+                cp16(smem_u32(dst), cla_ptr<float>(v, b, p, R * 4) + r * 4);
+            }
+        };
+        if (op.kind == kTipTip) {
+            cp16(smem_u32(sl.c), v.tips + (long long)op.c1 * v.npat_pad + (p & ~15));
+            cp16(smem_u32(sl.d), v.tips + (long long)op.c2 * v.npat_pad + (p & ~15));
+        } else {
+            slice(sl.a, op.c1, op.wide & kWideC1);
+            cp16(smem_u32(sl.c), v.scalers + (long long)op.c1 * v.npat_pad + (p & ~3));
+            if (op.kind == kIntInt) {
+                slice(sl.b, op.c2, op.wide & kWideC2);
+                cp16(smem_u32(sl.d), v.scalers + (long long)op.c2 * v.npat_pad + (p & ~3));
+            } else {
+                cp16(smem_u32(sl.d), v.tips + (long long)op.c2 * v.npat_pad + (p & ~15));
+            }
+        }
+    }
+    cp_commit();
+}
+
+// CLA update of tiles [t0, t1) of one op from prefetched inputs; the
+// arithmetic of cla_tiles_m
+template <int R>
+__device__ __forceinline__ void cla_tiles_cp(const View &v, const DevOp &op, const double *PL, const double *PR,
+                                             int t0, int t1, int r, bool lane_ok, unsigned char *cps) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    const int pl = threadIdx.x / G;
+#pragma unroll
+    for (int q = 0; q < kCpStages - 1; q++) cp_issue<R>(v, op, t0 + q, t1, r, lane_ok, cps, q);
+    int stage = 0;
+    for (int tile = t0; tile < t1; tile++) {
+        cp_issue<R>(v, op, tile + kCpStages - 1, t1, r, lane_ok, cps, stage == 0 ? kCpStages - 1 : stage - 1);
+        cp_wait<kCpStages - 1>();
+        const int p = tile * PPB + pl;
+        const bool act = lane_ok && p < v.npat;
+        double d[4] = {0, 0, 0, 0};
+        int m = 0;
+        if (act) {
+            const CpSlots sl = cp_slots(cps, stage);
+            auto slice = [&](const unsigned char *src, bool wide, double out[4]) {
+                if (wide || p < v.kpad) {
+                    const double2 x = *reinterpret_cast<const double2 *>(src);
+                    const double2 y = *reinterpret_cast<const double2 *>(src + 16);
+                    out[0] = x.x;
+                    out[1] = x.y;
+                    out[2] = y.x;
+                    out[3] = y.y;
+                } else {
+                    const float4 f = *reinterpret_cast<const float4 *>(src);
+                    out[0] = f.x;
+                    out[1] = f.y;
+                    out[2] = f.z;
+                    out[3] = f.w;
+                }
+            };
+            double a[4], b[4], x[4], y[4];
+            if (op.kind == kTipTip) {
+                pvec_tip(PL, sl.c[p & 15], x);
+                pvec_tip(PR, sl.d[p & 15], y);
+            } else {
+                slice(sl.a, op.wide & kWideC1, a);
+                m = reinterpret_cast<const int *>(sl.c)[p & 3];
+                pvec(PL, a, x);
+                if (op.kind == kIntInt) {
+                    slice(sl.b, op.wide & kWideC2, b);
+                    m += reinterpret_cast<const int *>(sl.d)[p & 3];
+                    pvec(PR, b, y);
+                } else {
+                    pvec_tip(PR, sl.d[p & 15], y);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = x[k] * y[k];
+        }
+        cla_finish_m<R>(v, op.dest, op.wide & kWideDest, p, r, act, d, m);
+        stage = stage == kCpStages - 1 ? 0 : stage + 1;
     }
 }
 
@@ -436,6 +554,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
     __shared__ double sE[8][3 * NC];  // one E table per warp
     __shared__ double sP[2][R][kPStride];
     __shared__ double sUU[32];  // U, U^-1 of the model
+    extern __shared__ __align__(128) unsigned char dsm[];  // CLA levels: cp_smem_bytes() of prefetch slots
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int cr = threadIdx.x % G;             // CLA lane: category
@@ -474,7 +593,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
                     }
                     __syncthreads();
                 }
-                cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, cla_ok);
+                cla_tiles_cp<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, cla_ok, dsm);
             }
             if (!grid_barrier(A.gs, v.status)) return;
             mark(kBtCmdDone, 0);

@@ -1567,8 +1567,11 @@ static void *batch4m_func(int R) {
 static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery, int tiles, int chunks,
                          bool use_graph) {
     void *func = I->mixed ? batch4m_func(I->R) : batch4_func(I->R, true);
+    // the precision form prefetches its CLA levels' inputs into dynamic shared memory
+    const size_t dsmem = I->mixed ? (size_t)cp_smem_bytes() : 0;
+    if (dsmem) GB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
     int per_sm = 0;
-    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, dsmem));
     if (per_sm < 1) {
         g_last_error = "batched pass kernel cannot be resident";
         return GB_ERROR_NO_RESOURCE;
@@ -1622,7 +1625,7 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(per_sm * I->nsm);
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = dsmem;
     cfg.stream = I->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;

@@ -44,8 +44,6 @@ struct TcShape {
     static constexpr int NP = (S + 15) / 16 * 16;  // N padded to a multiple of 16
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 __device__ __forceinline__ float to_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -94,21 +92,6 @@ __device__ __forceinline__ void tc_ld8_nw(uint32_t taddr, uint32_t r[8]) {
                  : "r"(taddr));
 }
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
-
-// bounded wait for the phase with the given parity; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (long long it = 0; it < (1LL << 24); it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, P1;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
 
 // Stage rows [p0, p0 + 128) of one child (CLA or tip) for category r as hi/lo
 // tf32 operands, four K-consecutive elements (one 16-byte core-matrix row
