@@ -577,7 +577,7 @@ def main():
                        "npat": w.data.npat, "candidates": len(conn), "moves": "SPR radius U{1..8} (1 = NNI)",
                        "model": "GTR+G4", "form": "batched precision (FP32 CLAs, pow2 scalers, FP64 Newton)",
                        "step": "one generation: dirty-CLA rescore + 3-branch Newton + final score per candidate",
-                       "cla_updates_per_step": cnt["cla_ops"], "l2": "working set > L2 (coefficients 1.2 GB)",
+                       "cla_updates_per_step": cnt["cla_ops"], "l2": "working set > L2 (coefficients 0.97 GB)",
                        "tuning": tuning, "parallelism": f"replicas{ws}"},
             "lnl_evals_per_s": edges / (ms / 1000.0),
             "plain_per_tree": {"value": plain_v, "unit": UNIT, "form": "plain FP64, per candidate, host Newton loop",
