@@ -546,6 +546,32 @@ __global__ void __launch_bounds__(kThreads, 2) k_cla4m(View v, LevelOps ops) {
         cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ntiles, t0 + kCla4mTiles), crr, ok);
 }
 
+// The CLA levels of a batched pass as launches of their own, one per level
+// ahead of the persistent kernel (same stream, same graph): the level code
+// alone fits 85 registers, so 3 CTAs share an SM instead of the persistent
+// kernel's 2 (its sweep and coefficient phases need 128).  blockIdx.y = the
+// op, blockIdx.x = a run of tpi tiles, inputs prefetched as in the persistent
+// kernel's levels.
+template <int R>
+__global__ void __launch_bounds__(kThreads, 3) k_level4m(View v, const DevOp *ops, int tpi) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    __shared__ double sP[2][R][kPStride];
+    extern __shared__ __align__(128) unsigned char dsm[];  // cp_smem_bytes() of prefetch slots
+    const DevOp op = ops[blockIdx.y];
+    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+        const int mi = q / (R * 16), rem = q % (R * 16);
+        sP[mi][rem / 16][rem % 16] = __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
+    }
+    __syncthreads();
+    const int cr = threadIdx.x % G;
+    const bool ok = cr < R;
+    const int crr = ok ? cr : 0;
+    const int ctiles = (v.npat + PPB - 1) / PPB;
+    const int t0 = blockIdx.x * tpi;
+    cla_tiles_cp<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, ok, dsm);
+}
+
 template <int R>
 __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
     constexpr int G = Lanes<R>::G;

@@ -1563,10 +1563,31 @@ static void *batch4m_func(int R) {
     }
 }
 
-// Enqueue one batched pass on the instance stream (no synchronisation).
+static void *level4m_func(int R) {
+    switch (R) {
+        case 1: return (void *)k_level4m<1>;
+        case 2: return (void *)k_level4m<2>;
+        case 3: return (void *)k_level4m<3>;
+        case 4: return (void *)k_level4m<4>;
+        case 5: return (void *)k_level4m<5>;
+        case 6: return (void *)k_level4m<6>;
+        case 7: return (void *)k_level4m<7>;
+        default: return (void *)k_level4m<8>;
+    }
+}
+
+// Enqueue one batched pass on the instance stream (no synchronisation).  The
+// precision form runs its leading CLA levels as k_level4m launches and the
+// rest of the command queue in the persistent kernel.
 static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery, int tiles, int chunks,
                          bool use_graph) {
     void *func = I->mixed ? batch4m_func(I->R) : batch4_func(I->R, true);
+    int nlev = 0;
+    if (I->mixed)
+        while (nlev < (int)P.cmds.size() && P.cmds[nlev].type == kBLevel) nlev++;
+    void *lfunc = I->mixed ? level4m_func(I->R) : nullptr;
+    if (lfunc)
+        GB_CUDA(cudaFuncSetAttribute(lfunc, cudaFuncAttributeMaxDynamicSharedMemorySize, cp_smem_bytes()));
     // the precision form prefetches its CLA levels' inputs into dynamic shared memory
     const size_t dsmem = I->mixed ? (size_t)cp_smem_bytes() : 0;
     if (dsmem) GB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
@@ -1579,8 +1600,8 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     View v = make_view(I);
     v.rescale_every = rescaleEvery;
     MixedArgs M;
-    M.cmds = I->d_bcmds;
-    M.ncmd = (int)P.cmds.size();
+    M.cmds = I->d_bcmds + nlev;
+    M.ncmd = (int)P.cmds.size() - nlev;
     M.ops = I->d_bops;
     M.entries = I->d_mentries;
     M.slots = I->d_bslots;
@@ -1632,6 +1653,26 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    // the whole pass on the stream: level launches, then the persistent kernel
+    // (none when the queue held levels only)
+    const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
+    const int ctiles = (I->npat + kThreads / G - 1) / (kThreads / G);
+    auto launch_all = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int l = 0; l < nlev && e == cudaSuccess; l++) {
+            const DevOp *ops = I->d_bops + P.cmds[l].a;
+            int tpi = tiles;
+            void *largs[] = {&v, (void *)&ops, &tpi};
+            e = cudaLaunchKernel(lfunc, dim3((ctiles + tiles - 1) / tiles, P.cmds[l].b), dim3(kThreads), largs,
+                                 cp_smem_bytes(), I->stream);
+        }
+        if (e == cudaSuccess && nlev < (int)P.cmds.size()) {
+            e = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream);
+            if (e == cudaSuccess) e = cudaLaunchKernelExC(&cfg, func, args);
+        }
+        return e;
+    };
+    const int nkernels = nlev + (nlev < (int)P.cmds.size() ? 1 : 0);
     const unsigned long long gkey = P.key ^ ((unsigned long long)tiles << 40) ^ ((unsigned long long)chunks << 48) ^
                                     ((unsigned long long)rescaleEvery << 56) ^
                                     (reinterpret_cast<unsigned long long>(I->d_trace) * 0x9E3779B97F4A7C15ULL);
@@ -1644,11 +1685,10 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
             I->bgraph_key = 0;
             bool ok = cudaStreamBeginCapture(I->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
             if (ok) {
-                const bool m = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream) == cudaSuccess;
-                const bool k = m && cudaLaunchKernelExC(&cfg, func, args) == cudaSuccess;
+                const bool k = launch_all() == cudaSuccess;
                 cudaGraph_t g = nullptr;
                 const bool e = cudaStreamEndCapture(I->stream, &g) == cudaSuccess;
-                ok = m && k && e && g;
+                ok = k && e && g;
                 if (ok && cudaGraphInstantiate(&I->bgraph_exec, g, 0) != cudaSuccess) ok = false;
                 if (ok) {
                     I->bgraph = g;
@@ -1665,13 +1705,12 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
         }
         if (I->bgraph_exec) {
             GB_CUDA(cudaGraphLaunch(I->bgraph_exec, I->stream));
-            I->launches += 1;
+            I->launches += nkernels;
             return GB_SUCCESS;
         }
     }
-    GB_CUDA(cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream));
-    GB_CUDA(cudaLaunchKernelExC(&cfg, func, args));
-    I->launches += 1;
+    GB_CUDA(launch_all());
+    I->launches += nkernels;
     return GB_SUCCESS;
 }
 
