@@ -1,33 +1,38 @@
-// gb_batch_mixed.cuh -- the precision form's batched candidate kernel.
+// gb_batch_mixed.cuh -- the precision form's batched candidate pass.
 //
-// Same command queue as k_batch4 (gb_batch.cuh), laid out for throughput:
-//   kBLevel : CLA updates with one lane per (pattern, category), the op's P
-//             blocks in padded shared memory, FP64 fused arithmetic, the
-//             pattern's power-of-two normalisation by a shuffle max, FP32
-//             stores with unbiased stochastic rounding (exact, no division);
-//             both children's loads are issued before any arithmetic.
-//   kBCoef  : for every candidate's step, the spectral coefficients of the
-//             branch it optimises.  With P_r(t) = U diag(exp(s_rk t)) U^-1,
-//             s_rk = lambda_k rate_r / (1 - pinv),
+// The command queue of k_batch4 (gb_batch.cuh), laid out for throughput and
+// run as one CUDA graph of three kernels:
+//   k_level4m (kBLevel, one launch per level): CLA updates with one lane per
+//             (pattern, category), the op's P blocks in padded shared memory,
+//             FP64 fused arithmetic, the pattern's power-of-two
+//             normalisation by a shuffle max, FP32 stores with unbiased
+//             stochastic rounding (exact, no division); every lane prefetches
+//             its inputs two tiles ahead with cp.async.
+//   k_coef4m  (kBCoef, one launch per step): for every candidate's step, the
+//             spectral coefficients of the branch it optimises.  With
+//             P_r(t) = U diag(exp(s_rk t)) U^-1, s_rk = lambda_k rate_r / (1 - pinv),
 //               L_p(t) = sum_rk A[p,r,k] exp(s_rk t) (+ the +I term), with
 //               A[p,r,k] = w_r (sum_i pi_i W[p,r,i] U[i,k]) (sum_j U^-1[k,j] V[p,r,j]),
 //             where W = (P_o1 V_o1) o (P_o2 V_o2) is the partial on the
 //             connector's side, formed in FP64 registers and never stored,
 //             and V the CLA (or tip) across the branch.  One lane per
-//             (pattern, category), loads first as in kBLevel.  A is FP64.
-//             A reversible rate matrix's rows sum to zero, so one eigenvalue
-//             lambda_k0 is zero (to rounding) and exp(s_rk0 t) = 1 for every
-//             category and length: its R coefficients are stored as one sum,
-//             1 + 3R per pattern, laid out [slot][q][pattern] with q = 0 the
-//             stationary sum and q = 1 + 3r + j the j-th other eigenvalue of
-//             category r; the site's scale exponent is m_o1 + m_o2 + m_V.
-//   kBNewton: Newton-Raphson in lockstep; an iteration reads only A:
+//             (pattern, category).  A is FP64.  A reversible rate matrix's
+//             rows sum to zero, so one eigenvalue lambda_k0 is zero (to
+//             rounding) and exp(s_rk0 t) = 1 for every category and length:
+//             its R coefficients are stored as one sum, 1 + 3R per pattern,
+//             laid out [slot][q][pattern] with q = 0 the stationary sum and
+//             q = 1 + 3r + j the j-th other eigenvalue of category r; the
+//             site's scale exponent is m_o1 + m_o2 + m_V.
+//   k_batch4m (the kBNewton / kBScore runs between them, persistent):
+//             Newton-Raphson in lockstep; an iteration reads only A:
 //             L = A_0 + sum A e, dL/dt = sum A s e, d2L/dt2 = sum A s^2 e with the
 //             per-candidate tables e, s e, s^2 e recomputed in FP64 after
 //             every step.  A chunk = 256 patterns summed by one warp (8 per
 //             lane, then a shuffle tree) -- no block barrier; the candidate's
-//             chunk sums are reduced by one warp in a fixed order.
-//   kBScore : the same sweep at the optimised lengths.
+//             chunk sums are reduced by one warp in a fixed order.  kBScore:
+//             the same sweep at the optimised lengths.
+// The level and coefficient kernels need ~80 registers a thread (3 CTAs per
+// SM); the persistent kernel's sweeps 120 (2 CTAs per SM).
 // lnL, d1, d2 accumulate in FP64; the Newton step and P(t) are FP64.
 #pragma once
 #include "gb_batch.cuh"
@@ -572,21 +577,38 @@ __global__ void __launch_bounds__(kThreads, 3) k_level4m(View v, const DevOp *op
     cla_tiles_cp<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, ok, dsm);
 }
 
+// A coefficient pass as a launch of its own, between the persistent kernel's
+// Newton commands: blockIdx.y = the entry, blockIdx.x = a run of tpi tiles.
+template <int R>
+__global__ void __launch_bounds__(kThreads, 3) k_coef4m(View v, MixedArgs A, int first_entry, int tpi) {
+    constexpr int G = Lanes<R>::G;
+    constexpr int PPB = kThreads / G;
+    __shared__ double sP[2][R][kPStride];
+    __shared__ double sUU[32];
+    const int e = blockIdx.y;
+    const MEntry en = A.entries[first_entry + e];
+    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+        const int mi = q / (R * 16), rem = q % (R * 16);
+        const int mat = mi ? en.m2 : en.m1;
+        sP[mi][rem / 16][rem % 16] = mat >= 0 ? __ldcg(v.mats + (long long)mat * v.mat_stride + rem) : 0.0;
+    }
+    for (int q = threadIdx.x; q < 32; q += blockDim.x) sUU[q] = __ldg(A.eig + 4 + q);
+    __syncthreads();
+    const int cr = threadIdx.x % G;
+    const bool ok = cr < R;
+    const int crr = ok ? cr : 0;
+    const int ctiles = (v.npat + PPB - 1) / PPB;
+    const int t0 = blockIdx.x * tpi;
+    coef_tiles_m<R>(v, A, en, en.m1 >= 0 ? sP[0][crr] : nullptr, en.m2 >= 0 ? sP[1][crr] : nullptr, sUU, sUU + 16, e,
+                    t0, min(ctiles, t0 + tpi), crr, ok, stationary_index(A.eig));
+}
+
 template <int R>
 __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
-    constexpr int G = Lanes<R>::G;
-    constexpr int PPB = kThreads / G;           // patterns per CLA tile
     constexpr int NC = Coefs<R>::N;
     __shared__ double sE[8][3 * NC];  // one E table per warp
-    __shared__ double sP[2][R][kPStride];
-    __shared__ double sUU[32];  // U, U^-1 of the model
-    extern __shared__ __align__(128) unsigned char dsm[];  // CLA levels: cp_smem_bytes() of prefetch slots
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int cr = threadIdx.x % G;             // CLA lane: category
-    const bool cla_ok = cr < R;
-    const int crr = cla_ok ? cr : 0;
-    const int ctiles = (v.npat + PPB - 1) / PPB;
     const int nchunks = (v.npat + 255) / 256;
     const int gwarp = blockIdx.x * (kThreads / 32) + warp;
     const int nwarps = gridDim.x * (kThreads / 32);
@@ -598,67 +620,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4m(View v, MixedArgs A) {
     };
     for (int ci = 0; ci < A.ncmd; ci++) {
         const BCmd cmd = A.cmds[ci];
-        mark(cmd.type == kBLevel ? kBtLevel : kBtNewton, cmd.b);
-        if (cmd.type == kBLevel) {
-            const int tpi = A.tiles_per_item;
-            const int items_per_op = (ctiles + tpi - 1) / tpi;
-            const long long nitems = (long long)cmd.b * items_per_op;
-            int cur = -1;
-            DevOp op;
-            for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-                const int j = (int)(item / items_per_op);
-                const int t0 = (int)(item % items_per_op) * tpi;
-                if (j != cur) {  // uniform across the block
-                    cur = j;
-                    op = A.ops[cmd.a + j];
-                    __syncthreads();
-                    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
-                        const int mi = q / (R * 16), rem = q % (R * 16);
-                        sP[mi][rem / 16][rem % 16] =
-                            __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
-                    }
-                    __syncthreads();
-                }
-                cla_tiles_cp<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, cla_ok, dsm);
-            }
-            if (!grid_barrier(A.gs, v.status)) return;
-            mark(kBtCmdDone, 0);
-            continue;
-        }
+        mark(kBtNewton, cmd.b);
         const int n = cmd.b;
         const MEntry *ents = A.entries + cmd.a;
         BSlot *slots = A.slots + cmd.a;
-        if (cmd.type == kBCoef) {
-            // work items = (entry, run of CLA-sized tiles); the entry's P blocks,
-            // U and U^-1 in shared memory
-            const int tpi = A.tiles_per_item;
-            const int items_per_entry = (ctiles + tpi - 1) / tpi;
-            const long long nitems = (long long)n * items_per_entry;
-            int loaded = -1;
-            MEntry en;
-            const int k0 = stationary_index(A.eig);
-            for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-                const int e = (int)(item / items_per_entry);
-                const int t0 = (int)(item % items_per_entry) * tpi;
-                if (e != loaded) {  // uniform across the block
-                    loaded = e;
-                    en = ents[e];
-                    __syncthreads();
-                    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
-                        const int mi = q / (R * 16), rem = q % (R * 16);
-                        const int mat = mi ? en.m2 : en.m1;
-                        sP[mi][rem / 16][rem % 16] = mat >= 0 ? __ldcg(v.mats + (long long)mat * v.mat_stride + rem) : 0.0;
-                    }
-                    for (int q = threadIdx.x; q < 32; q += blockDim.x) sUU[q] = __ldg(A.eig + 4 + q);
-                    __syncthreads();
-                }
-                coef_tiles_m<R>(v, A, en, en.m1 >= 0 ? sP[0][crr] : nullptr, en.m2 >= 0 ? sP[1][crr] : nullptr, sUU,
-                                sUU + 16, e, t0, min(ctiles, t0 + tpi), crr, cla_ok, k0);
-            }
-            if (!grid_barrier(A.gs, v.status)) return;
-            mark(kBtCmdDone, 0);
-            continue;
-        }
         const bool newton = cmd.type == kBNewton;
         // start: Newton states and e tables at the current lengths, everyone active
         for (int e = gwarp; e < n; e += nwarps) {

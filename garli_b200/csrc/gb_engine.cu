@@ -1563,6 +1563,19 @@ static void *batch4m_func(int R) {
     }
 }
 
+static void *coef4m_func(int R) {
+    switch (R) {
+        case 1: return (void *)k_coef4m<1>;
+        case 2: return (void *)k_coef4m<2>;
+        case 3: return (void *)k_coef4m<3>;
+        case 4: return (void *)k_coef4m<4>;
+        case 5: return (void *)k_coef4m<5>;
+        case 6: return (void *)k_coef4m<6>;
+        case 7: return (void *)k_coef4m<7>;
+        default: return (void *)k_coef4m<8>;
+    }
+}
+
 static void *level4m_func(int R) {
     switch (R) {
         case 1: return (void *)k_level4m<1>;
@@ -1577,8 +1590,9 @@ static void *level4m_func(int R) {
 }
 
 // Enqueue one batched pass on the instance stream (no synchronisation).  The
-// precision form runs its leading CLA levels as k_level4m launches and the
-// rest of the command queue in the persistent kernel.
+// precision form runs its leading CLA levels as k_level4m launches, each
+// coefficient pass as a k_coef4m launch, and every run of Newton / score
+// commands between them in the persistent kernel.
 static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery, int tiles, int chunks,
                          bool use_graph) {
     void *func = I->mixed ? batch4m_func(I->R) : batch4_func(I->R, true);
@@ -1588,11 +1602,8 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     void *lfunc = I->mixed ? level4m_func(I->R) : nullptr;
     if (lfunc)
         GB_CUDA(cudaFuncSetAttribute(lfunc, cudaFuncAttributeMaxDynamicSharedMemorySize, cp_smem_bytes()));
-    // the precision form prefetches its CLA levels' inputs into dynamic shared memory
-    const size_t dsmem = I->mixed ? (size_t)cp_smem_bytes() : 0;
-    if (dsmem) GB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
     int per_sm = 0;
-    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, dsmem));
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
     if (per_sm < 1) {
         g_last_error = "batched pass kernel cannot be resident";
         return GB_ERROR_NO_RESOURCE;
@@ -1646,7 +1657,7 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(per_sm * I->nsm);
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = dsmem;
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = I->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1657,6 +1668,7 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     // (none when the queue held levels only)
     const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
     const int ctiles = (I->npat + kThreads / G - 1) / (kThreads / G);
+    const int ncmd = (int)P.cmds.size();
     auto launch_all = [&]() -> cudaError_t {
         cudaError_t e = cudaSuccess;
         for (int l = 0; l < nlev && e == cudaSuccess; l++) {
@@ -1666,13 +1678,34 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
             e = cudaLaunchKernel(lfunc, dim3((ctiles + tiles - 1) / tiles, P.cmds[l].b), dim3(kThreads), largs,
                                  cp_smem_bytes(), I->stream);
         }
-        if (e == cudaSuccess && nlev < (int)P.cmds.size()) {
+        if (!I->mixed) {
+            if (e == cudaSuccess) e = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream);
+            if (e == cudaSuccess) e = cudaLaunchKernelExC(&cfg, func, args);
+            return e;
+        }
+        for (int c = nlev; c < ncmd && e == cudaSuccess;) {
+            if (P.cmds[c].type == kBCoef) {
+                int first = P.cmds[c].a, tpi = tiles;
+                void *cargs[] = {&v, &M, &first, &tpi};
+                e = cudaLaunchKernel(coef4m_func(I->R), dim3((ctiles + tiles - 1) / tiles, P.cmds[c].b),
+                                     dim3(kThreads), cargs, 0, I->stream);
+                c++;
+                continue;
+            }
+            int c1 = c;
+            while (c1 < ncmd && P.cmds[c1].type != kBCoef) c1++;
+            M.cmds = I->d_bcmds + c;
+            M.ncmd = c1 - c;
             e = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream);
             if (e == cudaSuccess) e = cudaLaunchKernelExC(&cfg, func, args);
+            c = c1;
         }
         return e;
     };
-    const int nkernels = nlev + (nlev < (int)P.cmds.size() ? 1 : 0);
+    int nkernels = nlev;
+    for (int c = nlev; c < ncmd; c++)
+        if (!I->mixed ? c == nlev : (P.cmds[c].type == kBCoef || c == nlev || P.cmds[c - 1].type == kBCoef))
+            nkernels++;
     const unsigned long long gkey = P.key ^ ((unsigned long long)tiles << 40) ^ ((unsigned long long)chunks << 48) ^
                                     ((unsigned long long)rescaleEvery << 56) ^
                                     (reinterpret_cast<unsigned long long>(I->d_trace) * 0x9E3779B97F4A7C15ULL);
