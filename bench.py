@@ -271,8 +271,10 @@ class _Null:
 
 
 def batch_kernel_roofline(r, args, peak, peak_kind):
-    """Achieved bandwidth of k_batch4m: algorithmic bytes of one launch over its
-    CUDA-event time on the instance stream (a few extra timed passes)."""
+    """Achieved bandwidth of the batched pass (one CUDA graph per generation:
+    k_level4m per CLA level, k_coef4m per step, k_batch4m for the Newton and
+    score runs): its algorithmic bytes over its CUDA-event time on the
+    instance stream (a few extra timed passes)."""
     import torch
 
     w_c3s = r["bw"]
@@ -291,10 +293,11 @@ def batch_kernel_roofline(r, args, peak, peak_kind):
     achieved = alg / (ms / 1e3) / 1e9
     traffic = profiled_traffic()
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic.get("bytes_per_launch") if traffic else None,
-            "kernel": "k_batch4m<4> (batched pass, one launch per generation)",
-            "peak_kind": f"{peak_kind} hbm_gbs (burst copy)", "kernel_ms_per_launch": ms,
-            "algorithmic_bytes_per_launch": alg,
+            "traffic": traffic.get("bytes_per_pass") if traffic else None,
+            "kernel": "batched pass: k_level4m<4> per CLA level, k_coef4m<4> per step, k_batch4m<4> per "
+                      "Newton run (one CUDA graph per generation)",
+            "peak_kind": f"{peak_kind} hbm_gbs (burst copy)", "ms_per_pass": ms,
+            "algorithmic_bytes_per_pass": alg,
             "traffic_note": traffic.get("note") if traffic else "no ncu capture committed"}
 
 

@@ -31,8 +31,8 @@
 //             lane, then a shuffle tree) -- no block barrier; the candidate's
 //             chunk sums are reduced by one warp in a fixed order.  kBScore:
 //             the same sweep at the optimised lengths.
-// The level and coefficient kernels need ~80 registers a thread (3 CTAs per
-// SM); the persistent kernel's sweeps 120 (2 CTAs per SM).
+// The level and coefficient kernels fit 64 registers a thread (4 CTAs per
+// SM); the persistent kernel's sweeps need 120 (2 CTAs per SM).
 // lnL, d1, d2 accumulate in FP64; the Newton step and P(t) are FP64.
 #pragma once
 #include "gb_batch.cuh"
@@ -211,12 +211,13 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
 // Prefetched CLA tiles: every lane copies its own inputs of the tiles ahead
 // into its own shared-memory slots with asynchronous copies (cp.async, 16
 // bytes, through L2), kCpStages - 1 tiles ahead of the arithmetic, so a lane
-// keeps several tiles' loads in flight without holding them in registers and
-// without block barriers (a lane reads only what it copied).  Per lane and
+// keeps the next tile's loads in flight without holding them in registers and
+// without block barriers (a lane reads only what it copied).  Two stages at 4
+// CTAs per SM measured faster than three at 3.  Per lane and
 // stage: child 1's slice (32 B), child 2's slice (32 B), and two 16-byte
 // words holding the pattern's scale exponent or tip code (the aligned
 // 16-byte block that contains it).  Layout [stage][field][lane].
-constexpr int kCpStages = 3;
+constexpr int kCpStages = 2;
 constexpr int kCpLane = 96;  // bytes per lane and stage
 __host__ __device__ constexpr int cp_smem_bytes() { return kCpStages * kCpLane * kThreads; }
 
@@ -553,12 +554,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_cla4m(View v, LevelOps ops) {
 
 // The CLA levels of a batched pass as launches of their own, one per level
 // ahead of the persistent kernel (same stream, same graph): the level code
-// alone fits 85 registers, so 3 CTAs share an SM instead of the persistent
-// kernel's 2 (its sweep and coefficient phases need 128).  blockIdx.y = the
+// alone fits 64 registers, so 4 CTAs share an SM instead of the persistent
+// kernel's 2 (its sweeps need 120).  blockIdx.y = the
 // op, blockIdx.x = a run of tpi tiles, inputs prefetched as in the persistent
 // kernel's levels.
 template <int R>
-__global__ void __launch_bounds__(kThreads, 3) k_level4m(View v, const DevOp *ops, int tpi) {
+__global__ void __launch_bounds__(kThreads, 4) k_level4m(View v, const DevOp *ops, int tpi) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     __shared__ double sP[2][R][kPStride];
@@ -580,7 +581,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_level4m(View v, const DevOp *op
 // A coefficient pass as a launch of its own, between the persistent kernel's
 // Newton commands: blockIdx.y = the entry, blockIdx.x = a run of tpi tiles.
 template <int R>
-__global__ void __launch_bounds__(kThreads, 3) k_coef4m(View v, MixedArgs A, int first_entry, int tpi) {
+__global__ void __launch_bounds__(kThreads, 4) k_coef4m(View v, MixedArgs A, int first_entry, int tpi) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     __shared__ double sP[2][R][kPStride];
