@@ -99,6 +99,28 @@ __device__ __forceinline__ float round_stochastic_exact(double x, unsigned int k
     return u < frac ? hi : lo;
 }
 
+// Unbiased stochastic rounding of a slice's four non-negative finite doubles
+// to float, for the DNA CLA stores: value k goes to its upper float neighbour
+// with probability (x - lo) / (hi - lo), its uniform variate the k-th 16-bit
+// field of one 64-bit hash of `key` (the SplitMix64 finalizer).  hi - lo is a
+// power of two and x - lo is exact, so u (hi - lo) < (x - lo) 2^16 is an exact
+// test (no division); the 16-bit variates round up at most 2^-16 ulp too often.
+__device__ __forceinline__ float4 round_stochastic4(const double d[4], unsigned int key) {
+    unsigned long long h = (unsigned long long)key * 0x9E3779B97F4A7C15ULL;
+    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    h = (h ^ (h >> 27)) * 0x94D049BB133111EBULL;
+    h ^= h >> 31;
+    float o[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float lo = __double2float_rz(d[k]);
+        const float hi = __uint_as_float(__float_as_uint(lo) + 1);
+        const double u = (double)(unsigned int)((h >> (16 * k)) & 0xffffu);
+        o[k] = (isfinite(hi) && u * ((double)hi - (double)lo) < (d[k] - (double)lo) * 65536.0) ? hi : lo;
+    }
+    return make_float4(o[0], o[1], o[2], o[3]);
+}
+
 // Power-of-two normalisation of one pattern-category slice d[4] (the max over
 // the pattern's G lanes) and its store: FP64 segment as is, FP32 segment with
 // stochastic rounding.  All G lanes of the pattern must call this together.
@@ -121,10 +143,8 @@ __device__ __forceinline__ void cla_finish_m(const View &v, int dest, bool wide,
         st4d(cla_ptr<double>(v, dest, p, R * 4) + r * 4, d);
     } else {
         float *q = cla_ptr<float>(v, dest, p, R * 4) + r * 4;
-        const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(q) >> 2);
-        reinterpret_cast<float4 *>(q)[0] =
-            make_float4(round_stochastic_exact(d[0], key), round_stochastic_exact(d[1], key + 1),
-                        round_stochastic_exact(d[2], key + 2), round_stochastic_exact(d[3], key + 3));
+        const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(q) >> 4);
+        reinterpret_cast<float4 *>(q)[0] = round_stochastic4(d, key);
     }
     if (r == 0) v.scalers[(long long)dest * v.npat_pad + p] = m - e;
 }
