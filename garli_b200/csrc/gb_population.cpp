@@ -15,7 +15,10 @@
 // computed once; a candidate needs D(A <- X), D(B <- X), D(C <- X) for the
 // connector X with neighbours A = X->left, B = X->right, C = X->anc, and only
 // the keys not already present become CLA updates.  Identical subtrees are
-// shared across candidates too.  Per step the partial on X's side of the
+// shared across candidates too.  A candidate keeps the base tree's node
+// numbers, so only the subtrees a move changed (the nodes whose children or
+// child lengths differ, and their ancestors) are hashed; the wanted CLAs are
+// looked up from the top and only a missing one's sides are descended into.  Per step the partial on X's side of the
 // optimised branch (D(X <- A), D(X <- C), D(X <- B)) is recomputed from the
 // branches optimised before it.
 //
@@ -144,6 +147,12 @@ struct Pop {
     long long c_ops = 0, c_updates = 0, c_evals = 0, c_base_ops = 0, c_edges = 0;
     double c_bytes = 0.0;
     int npat = 0, ncat = 1;
+    std::vector<Key> base_down;  // key of every node's subtree in the base tree (rooted at node 0)
+    Topo cand;                   // the candidate being planned (storage reused)
+    std::vector<Key> down;       // its subtree keys
+    std::vector<char> changed;   // its subtrees that differ from the base's
+    std::vector<Key> up;         // up[u]: D(anc u <- u), the rest of the tree seen from u's parent
+    std::vector<char> up_known;
 };
 
 std::mutex g_mu;
@@ -233,6 +242,107 @@ Made need_key(Pop &p, const Topo &t, int v, int u, std::vector<gb_cla_operation>
     return {key, made};
 }
 
+// Keys of every node's subtree (the CLA D(v <- anc v)), the same keys
+// need_key computes.  base_keys: every node of the base tree, post-order from
+// the root.  cand_keys: a candidate with the base's node numbering -- a node
+// whose children or child branch lengths differ from the base's is changed,
+// and so is every ancestor of it; only changed nodes are hashed, the others
+// keep the base's key.
+void hash_node(const Topo &t, int v, std::vector<Key> &down) {
+    Key terms[3];
+    int k = 0;
+    for (int c : {t.left[v], t.mid[v], t.right[v]})
+        if (c >= 0) terms[k++] = term(down[c], t.dlen[c]);
+    // the root's key (three children) is never used as a CLA key
+    down[v] = k == 2 ? combine(terms[0], terms[1]) : combine(combine(terms[0], terms[1]), terms[2]);
+}
+void keys_below(const Topo &t, int v, const std::vector<char> *changed, std::vector<Key> &down) {
+    for (int c : {t.left[v], t.mid[v], t.right[v]})
+        if (c >= 0 && !t.tip(c) && (!changed || (*changed)[c])) keys_below(t, c, changed, down);
+    if (v != 0) hash_node(t, v, down);
+}
+void base_keys(const Topo &t, std::vector<Key> &down) {
+    down.resize(t.nnodes);
+    for (int v = 1; v <= t.ntax; v++) down[v] = tip_key(v);
+    keys_below(t, 0, nullptr, down);
+}
+void cand_keys(Pop &p, const Topo &t) {
+    const Topo &b = p.base;
+    const int N = t.nnodes;
+    p.down = p.base_down;
+    p.changed.assign(N, 0);
+    auto mark = [&](int v) {
+        for (int w = v; w >= 0 && !p.changed[w]; w = t.anc[w]) p.changed[w] = 1;
+    };
+    for (int v = 0; v < N; v++) {
+        if (t.left[v] != b.left[v] || t.right[v] != b.right[v] || t.mid[v] != b.mid[v]) mark(v);
+        if (v > 0 && bits(t.dlen[v]) != bits(b.dlen[v])) mark(t.anc[v]);
+    }
+    if (p.changed[0]) keys_below(t, 0, &p.changed, p.down);
+    p.up.resize(N);
+    p.up_known.assign(N, 0);
+}
+
+// key of D(v <- u) in the candidate: v's subtree when u is v's parent, else
+// (u a child of v) the rest of the tree seen from v, built up the path to the
+// root (each such key once per candidate)
+Key dir_key(Pop &p, const Topo &t, int v, int u) {
+    if (t.tip(v) || t.anc[v] == u) return p.down[v];
+    if (p.up_known[u]) return p.up[u];
+    Key terms[2];
+    int k = 0;
+    if (t.anc[v] >= 0) terms[k++] = term(dir_key(p, t, t.anc[v], v), t.dlen[v]);
+    for (int c : {t.left[v], t.mid[v], t.right[v]})
+        if (c >= 0 && c != u && k < 2) terms[k++] = term(p.down[c], t.dlen[c]);
+    p.up[u] = combine(terms[0], terms[1]);
+    p.up_known[u] = 1;
+    return p.up[u];
+}
+
+// need_key for a candidate with its keys known: look D(v <- u) up first and
+// descend only into the sides of a CLA that is missing
+Made need_dir(Pop &p, const Topo &t, int v, int u, std::vector<gb_cla_operation> &ops, int *rc) {
+    if (t.tip(v)) return {tip_key(v), {v - 1, 0}};
+    const Key key = dir_key(p, t, v, u);
+    auto it = p.cla.find(key);
+    if (it != p.cla.end()) return {key, it->second};
+    int nb[3];
+    double ln[3];
+    const int k = t.nbrs(v, nb, ln);
+    int ch[2], c = 0;
+    double cl[2];
+    for (int i = 0; i < k; i++)
+        if (nb[i] != u && c < 2) {
+            ch[c] = nb[i];
+            cl[c++] = ln[i];
+        }
+    if (c != 2 || k != 3) {
+        *rc = GB_ERROR_OUT_OF_RANGE;
+        return {{0, 0}, {0, 0}};
+    }
+    const Made a = need_dir(p, t, ch[0], v, ops, rc);
+    if (*rc) return a;
+    const Made b = need_dir(p, t, ch[1], v, ops, rc);
+    if (*rc) return b;
+    if (p.next_buf + 1 > p.ntip + p.nbuf) {
+        *rc = GB_ERROR_OUT_OF_RANGE;
+        return {key, {0, 0}};
+    }
+    Cla made;
+    made.buf = p.next_buf++;
+    made.level = (a.cla.level > b.cla.level ? a.cla.level : b.cla.level) + 1;
+    gb_cla_operation op;
+    op.destClaIndex = made.buf;
+    op.childClaIndex1 = a.cla.buf;
+    op.childClaIndex2 = b.cla.buf;
+    op.transMatIndex1 = mat_slot(p, cl[0], rc);
+    op.transMatIndex2 = mat_slot(p, cl[1], rc);
+    op.opDepLevel = made.level;
+    ops.push_back(op);
+    p.cla[key] = made;
+    return {key, made};
+}
+
 // every directional CLA of the base tree, computed once and kept.  wide: in
 // FP64 buffers (precision form, batched pass) -- they are shared by every
 // candidate, so their storage error would otherwise enter every candidate's lnL.
@@ -260,6 +370,7 @@ int prepare_base(Pop &p, bool wide) {
     if (rc) return rc;
     p.base_bufs = p.next_buf;
     p.base_mats = p.next_mat;
+    base_keys(p.base, p.base_down);
     std::vector<gb_transmat_operation> tops;
     for (int m = 0; m < p.next_mat; m++) tops.push_back({m, p.mat_len[m], 0, 1});
     if ((rc = gb_update_transition_matrices(p.inst, tops.data(), (int)tops.size()))) return rc;
@@ -307,18 +418,19 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
     P.nr_mat.resize(3 * nC);
     std::vector<int> wbuf(nC);
     for (int c = 0; c < nC; c++) {
-        Topo t;
+        Topo &t = p.cand;
         int rc = load_topo(t, p.base.ntax, child3s + (size_t)c * 3 * N, dlens + (size_t)c * N);
         if (rc) return rc;
         const int X = connectors[c];
         if (X <= t.ntax || X >= N || t.anc[X] < 0) return GB_ERROR_OUT_OF_RANGE;
+        cand_keys(p, t);
         const int A = t.left[X], B = t.right[X], Cn = t.anc[X];
         const size_t before = P.ops.size();
-        const Made va = need_key(p, t, A, X, P.ops, &rc);
+        const Made va = need_dir(p, t, A, X, P.ops, &rc);
         if (rc) return rc;
-        const Made vb = need_key(p, t, B, X, P.ops, &rc);
+        const Made vb = need_dir(p, t, B, X, P.ops, &rc);
         if (rc) return rc;
-        const Made vc = need_key(p, t, Cn, X, P.ops, &rc);
+        const Made vc = need_dir(p, t, Cn, X, P.ops, &rc);
         if (rc) return rc;
         for (size_t i = before; i < P.ops.size(); i++) P.op_owner.push_back(c);
         // the three branches get their own matrix slots: the device rewrites them
@@ -354,11 +466,7 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
 }
 
 // Algorithmic device-memory bytes of one batched pass of the precision form
-// per pattern (R = 4 categories): a CLA read is 64 B + a 4 B scaler (FP32),
-// 128 + 4 B when it is an FP64 parent-tree buffer, 1 B for a tip; a CLA
-// update writes 64 + 4 B; a coefficient pattern writes 128 + 4 B; an edge
-// evaluation pattern reads 128 + 4 + 4 + 4 B (coefficients, scale, count,
-// constant state).  See gbp_get_counters.
+// (see gbp_get_counters).
 double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps) {
     // per pattern: a CLA slice is 4R FP32 values and a 4-byte scale exponent
     // (FP64 values for the parent tree's wide buffers), a tip one byte; a
