@@ -502,6 +502,11 @@ class Population:
         return {"cla_ops": int(out[0]), "pattern_updates": int(out[1]), "deriv_evals": int(out[2]),
                 "base_cla_ops": int(out[3]), "edge_evals": int(out[4]), "alg_bytes": int(out[5])}
 
+    def set_tuning(self, tiles_per_item: int, chunks_per_item: int):
+        """Work-item sizes of the batched pass (0, 0: autotune on the next call)."""
+        _chk(lib().gb_set_batch_tuning(self.inst.h, int(tiles_per_item), int(chunks_per_item)),
+             "gb_set_batch_tuning")
+
     def batch_timing(self) -> dict:
         out = np.zeros(2)
         _chk(lib().gb_get_batch_timing(self.inst.h, _p(out, C.c_double)), "gb_get_batch_timing")

@@ -90,6 +90,22 @@ def test_batched_precision_form_matches_oracle_and_repeats(case):
     assert 1 <= per <= 60
 
 
+def test_batched_precision_form_does_not_depend_on_work_item_sizes(case):
+    """Tiles per item size the level and coefficient launches and the chunks
+    per item the Newton sweeps' work items; every reduction has a fixed
+    partition, so any choice gives bit-identical results."""
+    w, c3s, dls, conn, _ = case
+    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), mixed=True)
+    runs = []
+    for tiles, chunks in ((1, 1), (4, 2), (32, 4), (5, 3)):
+        pop.set_tuning(tiles, chunks)
+        runs.append(pop.score(c3s, dls, conn, 0.01))
+    for out, lens in runs[1:]:
+        assert np.array_equal(out, runs[0][0]) and np.array_equal(lens, runs[0][1])
+    pop.close()
+    inst.close()
+
+
 def test_population_switches_between_batched_and_per_tree_modes(case):
     """One precision-form population: batched (parent tree in FP64 buffers), then
     per-tree (parent rebuilt in ordinary buffers), then batched again."""
