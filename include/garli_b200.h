@@ -226,7 +226,10 @@ int gb_set_tensor_core_correction(int instance, double ulps);
  * A GA generation's candidates (population.cpp:4532-4589: each mutated
  * individual is rescored, tree.cpp:4003, and the branches around its move are
  * optimised, optimization.cpp:882-884 -> NewtonRaphsonOptimizeBranchLength,
- * :1359-1971) run as one persistent kernel over a device command queue.
+ * :1359-1971) run from a device command queue as one CUDA graph: the
+ * precision form's CLA levels and per-step coefficient passes as launches of
+ * their own, its lockstep Newton runs (and the plain form's whole queue) in a
+ * persistent kernel.
  * ops[0..opCount): every candidate's dirty CLA updates, levelled by opDepLevel
  * (uneven counts per candidate are fine; buffers may be shared read-only).
  * steps[c * stepsPerCandidate + k]: step k of candidate c -- optionally the CLA
