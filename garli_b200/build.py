@@ -51,11 +51,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     cmd = [
-        nvcc(), GENCODE, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O2",
+        nvcc(), GENCODE, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O2,-fopenmp",
         "-Xptxas", "-v" if verbose else "-O3",
         "-I", os.path.join(ROOT, "include"),
         "-o", LIB + ".tmp",
-    ] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart"]
+    ] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart", "-lgomp"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)

@@ -18,7 +18,9 @@
 // shared across candidates too.  A candidate keeps the base tree's node
 // numbers, so only the subtrees a move changed (the nodes whose children or
 // child lengths differ, and their ancestors) are hashed; the wanted CLAs are
-// looked up from the top and only a missing one's sides are descended into.  Per step the partial on X's side of the
+// looked up from the top and only a missing one's sides are descended into.
+// That part runs in parallel over candidates; buffers and updates are then
+// assigned in candidate order.  Per step the partial on X's side of the
 // optimised branch (D(X <- A), D(X <- C), D(X <- B)) is recomputed from the
 // branches optimised before it.
 //
@@ -129,6 +131,23 @@ struct Cla {
     int level;  // dependency level of the op that made it (0: tip or already computed)
 };
 
+// a CLA a candidate needs that the base tree does not hold, after its
+// children's: its key, its children's keys (or tip buffers) and branch lengths
+struct Miss {
+    Key key, k1, k2;
+    int tip1, tip2;  // the child's tip buffer, or -1
+    double l1, l2;
+};
+// what a candidate needs: its connector's three sides (A, C, B) and the
+// missing CLAs, children first
+struct CandNeed {
+    int rc = GB_SUCCESS;
+    Key side_key[3];
+    int side_tip[3];
+    double side_len[3];
+    std::vector<Miss> miss;
+};
+
 struct Pop {
     int inst = -1;
     int ntip = 0, nbuf = 0, nmat = 0;
@@ -148,11 +167,7 @@ struct Pop {
     double c_bytes = 0.0;
     int npat = 0, ncat = 1;
     std::vector<Key> base_down;  // key of every node's subtree in the base tree (rooted at node 0)
-    Topo cand;                   // the candidate being planned (storage reused)
-    std::vector<Key> down;       // its subtree keys
-    std::vector<char> changed;   // its subtrees that differ from the base's
-    std::vector<Key> up;         // up[u]: D(anc u <- u), the rest of the tree seen from u's parent
-    std::vector<char> up_known;
+    std::vector<CandNeed> needs; // planning storage, one per candidate (reused)
 };
 
 std::mutex g_mu;
@@ -266,46 +281,59 @@ void base_keys(const Topo &t, std::vector<Key> &down) {
     for (int v = 1; v <= t.ntax; v++) down[v] = tip_key(v);
     keys_below(t, 0, nullptr, down);
 }
-void cand_keys(Pop &p, const Topo &t) {
-    const Topo &b = p.base;
+// per-thread working storage for one candidate's keys
+struct CandScratch {
+    Topo t;
+    std::vector<Key> down, up;   // subtree keys; up[u] = D(anc u <- u)
+    std::vector<char> changed, up_known;
+};
+
+void cand_keys(const Pop &p, CandScratch &s) {
+    const Topo &b = p.base, &t = s.t;
     const int N = t.nnodes;
-    p.down = p.base_down;
-    p.changed.assign(N, 0);
+    s.down = p.base_down;
+    s.changed.assign(N, 0);
     auto mark = [&](int v) {
-        for (int w = v; w >= 0 && !p.changed[w]; w = t.anc[w]) p.changed[w] = 1;
+        for (int w = v; w >= 0 && !s.changed[w]; w = t.anc[w]) s.changed[w] = 1;
     };
     for (int v = 0; v < N; v++) {
         if (t.left[v] != b.left[v] || t.right[v] != b.right[v] || t.mid[v] != b.mid[v]) mark(v);
         if (v > 0 && bits(t.dlen[v]) != bits(b.dlen[v])) mark(t.anc[v]);
     }
-    if (p.changed[0]) keys_below(t, 0, &p.changed, p.down);
-    p.up.resize(N);
-    p.up_known.assign(N, 0);
+    if (s.changed[0]) keys_below(t, 0, &s.changed, s.down);
+    s.up.resize(N);
+    s.up_known.assign(N, 0);
 }
 
 // key of D(v <- u) in the candidate: v's subtree when u is v's parent, else
 // (u a child of v) the rest of the tree seen from v, built up the path to the
 // root (each such key once per candidate)
-Key dir_key(Pop &p, const Topo &t, int v, int u) {
-    if (t.tip(v) || t.anc[v] == u) return p.down[v];
-    if (p.up_known[u]) return p.up[u];
+Key dir_key(CandScratch &s, int v, int u) {
+    const Topo &t = s.t;
+    if (t.tip(v) || t.anc[v] == u) return s.down[v];
+    if (s.up_known[u]) return s.up[u];
     Key terms[2];
     int k = 0;
-    if (t.anc[v] >= 0) terms[k++] = term(dir_key(p, t, t.anc[v], v), t.dlen[v]);
+    if (t.anc[v] >= 0) terms[k++] = term(dir_key(s, t.anc[v], v), t.dlen[v]);
     for (int c : {t.left[v], t.mid[v], t.right[v]})
-        if (c >= 0 && c != u && k < 2) terms[k++] = term(p.down[c], t.dlen[c]);
-    p.up[u] = combine(terms[0], terms[1]);
-    p.up_known[u] = 1;
-    return p.up[u];
+        if (c >= 0 && c != u && k < 2) terms[k++] = term(s.down[c], t.dlen[c]);
+    s.up[u] = combine(terms[0], terms[1]);
+    s.up_known[u] = 1;
+    return s.up[u];
 }
 
-// need_key for a candidate with its keys known: look D(v <- u) up first and
-// descend only into the sides of a CLA that is missing
-Made need_dir(Pop &p, const Topo &t, int v, int u, std::vector<gb_cla_operation> &ops, int *rc) {
-    if (t.tip(v)) return {tip_key(v), {v - 1, 0}};
-    const Key key = dir_key(p, t, v, u);
-    auto it = p.cla.find(key);
-    if (it != p.cla.end()) return {key, it->second};
+// D(v <- u): its key (or tip buffer); if the base lacks it, its sides first,
+// then itself appended to cn.miss (base lookups only: read-only)
+void collect(const Pop &p, CandScratch &s, int v, int u, CandNeed &cn, Key &key, int &tip) {
+    const Topo &t = s.t;
+    if (t.tip(v)) {
+        key = tip_key(v);
+        tip = v - 1;
+        return;
+    }
+    tip = -1;
+    key = dir_key(s, v, u);
+    if (p.cla.count(key)) return;
     int nb[3];
     double ln[3];
     const int k = t.nbrs(v, nb, ln);
@@ -317,30 +345,16 @@ Made need_dir(Pop &p, const Topo &t, int v, int u, std::vector<gb_cla_operation>
             cl[c++] = ln[i];
         }
     if (c != 2 || k != 3) {
-        *rc = GB_ERROR_OUT_OF_RANGE;
-        return {{0, 0}, {0, 0}};
+        cn.rc = GB_ERROR_OUT_OF_RANGE;
+        return;
     }
-    const Made a = need_dir(p, t, ch[0], v, ops, rc);
-    if (*rc) return a;
-    const Made b = need_dir(p, t, ch[1], v, ops, rc);
-    if (*rc) return b;
-    if (p.next_buf + 1 > p.ntip + p.nbuf) {
-        *rc = GB_ERROR_OUT_OF_RANGE;
-        return {key, {0, 0}};
-    }
-    Cla made;
-    made.buf = p.next_buf++;
-    made.level = (a.cla.level > b.cla.level ? a.cla.level : b.cla.level) + 1;
-    gb_cla_operation op;
-    op.destClaIndex = made.buf;
-    op.childClaIndex1 = a.cla.buf;
-    op.childClaIndex2 = b.cla.buf;
-    op.transMatIndex1 = mat_slot(p, cl[0], rc);
-    op.transMatIndex2 = mat_slot(p, cl[1], rc);
-    op.opDepLevel = made.level;
-    ops.push_back(op);
-    p.cla[key] = made;
-    return {key, made};
+    Miss m;
+    m.key = key;
+    m.l1 = cl[0];
+    m.l2 = cl[1];
+    collect(p, s, ch[0], v, cn, m.k1, m.tip1);
+    collect(p, s, ch[1], v, cn, m.k2, m.tip2);
+    cn.miss.push_back(m);
 }
 
 // every directional CLA of the base tree, computed once and kept.  wide: in
@@ -410,38 +424,85 @@ struct Plan {
     std::vector<int> nr_mat;                  // 3 per candidate (X->left, X, X->right order)
 };
 
-// steps in GARLI's order: nd->left, nd, nd->right (optimization.cpp:882-884)
+// Steps in GARLI's order: nd->left, nd, nd->right (optimization.cpp:882-884).
+// Two phases: every candidate's keys and the CLAs the base tree lacks, in
+// parallel over candidates (read-only on the base); then, in candidate order,
+// the buffers, matrices and updates -- a CLA another candidate already made in
+// this call is shared.  The plan is the one a serial pass would build.
 int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const int *connectors, Plan &P) {
     const int N = p.base.nnodes;
     P.step_ops.resize(3 * nC);
     P.steps.resize(3 * nC);
     P.nr_mat.resize(3 * nC);
-    std::vector<int> wbuf(nC);
+    std::vector<CandNeed> &needs = p.needs;
+    needs.resize(nC);
+#pragma omp parallel for schedule(static) if (nC >= 16)
     for (int c = 0; c < nC; c++) {
-        Topo &t = p.cand;
-        int rc = load_topo(t, p.base.ntax, child3s + (size_t)c * 3 * N, dlens + (size_t)c * N);
-        if (rc) return rc;
+        thread_local CandScratch s;
+        CandNeed &cn = needs[c];
+        cn.rc = GB_SUCCESS;
+        cn.miss.clear();
+        cn.rc = load_topo(s.t, p.base.ntax, child3s + (size_t)c * 3 * N, dlens + (size_t)c * N);
+        if (cn.rc) continue;
+        const Topo &t = s.t;
         const int X = connectors[c];
-        if (X <= t.ntax || X >= N || t.anc[X] < 0) return GB_ERROR_OUT_OF_RANGE;
-        cand_keys(p, t);
-        const int A = t.left[X], B = t.right[X], Cn = t.anc[X];
-        const size_t before = P.ops.size();
-        const Made va = need_dir(p, t, A, X, P.ops, &rc);
-        if (rc) return rc;
-        const Made vb = need_dir(p, t, B, X, P.ops, &rc);
-        if (rc) return rc;
-        const Made vc = need_dir(p, t, Cn, X, P.ops, &rc);
-        if (rc) return rc;
-        for (size_t i = before; i < P.ops.size(); i++) P.op_owner.push_back(c);
+        if (X <= t.ntax || X >= N || t.anc[X] < 0) {
+            cn.rc = GB_ERROR_OUT_OF_RANGE;
+            continue;
+        }
+        cand_keys(p, s);
+        const int side[3] = {t.left[X], t.anc[X], t.right[X]};  // A, C, B
+        for (int k : {0, 2, 1})  // made in the order A, B, C
+            if (!cn.rc) collect(p, s, side[k], X, cn, cn.side_key[k], cn.side_tip[k]);
+        cn.side_len[0] = t.dlen[t.left[X]];
+        cn.side_len[1] = t.dlen[X];
+        cn.side_len[2] = t.dlen[t.right[X]];
+    }
+    auto find = [&](const Key &key, int tip, Cla &out) -> bool {
+        if (tip >= 0) {
+            out = {tip, 0};
+            return true;
+        }
+        auto it = p.cla.find(key);
+        if (it == p.cla.end()) return false;
+        out = it->second;
+        return true;
+    };
+    for (int c = 0; c < nC; c++) {
+        const CandNeed &cn = needs[c];
+        if (cn.rc) return cn.rc;
+        int rc = GB_SUCCESS;
+        for (const Miss &m : cn.miss) {
+            if (p.cla.count(m.key)) continue;  // made by an earlier candidate of this call
+            Cla a, b;
+            if (!find(m.k1, m.tip1, a) || !find(m.k2, m.tip2, b)) return GB_ERROR_OUT_OF_RANGE;
+            if (p.next_buf + 1 > p.ntip + p.nbuf) return GB_ERROR_OUT_OF_RANGE;
+            Cla made;
+            made.buf = p.next_buf++;
+            made.level = (a.level > b.level ? a.level : b.level) + 1;
+            gb_cla_operation op;
+            op.destClaIndex = made.buf;
+            op.childClaIndex1 = a.buf;
+            op.childClaIndex2 = b.buf;
+            op.transMatIndex1 = mat_slot(p, m.l1, &rc);
+            op.transMatIndex2 = mat_slot(p, m.l2, &rc);
+            op.opDepLevel = made.level;
+            if (rc) return rc;
+            P.ops.push_back(op);
+            P.op_owner.push_back(c);
+            p.cla[m.key] = made;
+        }
+        Cla sides[3];
+        for (int k = 0; k < 3; k++)
+            if (!find(cn.side_key[k], cn.side_tip[k], sides[k])) return GB_ERROR_OUT_OF_RANGE;
         // the three branches get their own matrix slots: the device rewrites them
-        const int mA = fresh_mat(p, t.dlen[A], &rc), mC = fresh_mat(p, t.dlen[X], &rc),
-                  mB = fresh_mat(p, t.dlen[B], &rc);
+        const int mA = fresh_mat(p, cn.side_len[0], &rc), mC = fresh_mat(p, cn.side_len[1], &rc),
+                  mB = fresh_mat(p, cn.side_len[2], &rc);
         if (rc) return rc;
         if (p.next_buf >= p.ntip + p.nbuf) return GB_ERROR_OUT_OF_RANGE;
         const int w = p.next_buf++;  // one partial buffer per candidate, rewritten at every step
-        wbuf[c] = w;
         // (child buffer, its matrix) of the three sides
-        const int sideBuf[3] = {va.cla.buf, vc.cla.buf, vb.cla.buf};
+        const int sideBuf[3] = {sides[0].buf, sides[1].buf, sides[2].buf};
         const int sideMat[3] = {mA, mC, mB};
         for (int k = 0; k < 3; k++) {
             const int o1 = (k + 1) % 3, o2 = (k + 2) % 3;  // the two other sides
