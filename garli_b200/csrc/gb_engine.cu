@@ -1838,7 +1838,6 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         c.b = (int)lv.size();
         P.ops.insert(P.ops.end(), lv.begin(), lv.end());
         P.cmds.push_back(c);
-        key = fnv(key, lv.data(), sizeof(DevOp) * lv.size());
     };
     if (rc == GB_SUCCESS)
         for (auto &lv : levels) add_level(lv);
@@ -1886,7 +1885,6 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         nc.type = kBNewton;
         P.cmds.push_back(nc);
     }
-    if (I->mixed) key = fnv(key, P.mentries.data(), sizeof(MEntry) * P.mentries.size());
     for (int k = 0; k < K && rc == GB_SUCCESS && !I->mixed && nC > 0; k++) {
         std::vector<gb_cla_operation> sops;
         for (int c = 0; c < nC; c++)
@@ -1926,8 +1924,14 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         P.cmds.push_back(fs);
     }
     P.max_entries = nC;
-    key = fnv(key, P.entries.data(), sizeof(BEntry) * P.entries.size());
+    // key of the captured graph: what its launches take as arguments -- the
+    // command list (level and entry counts, offsets), the candidate count, the
+    // Newton parameters and the instance's data version; the ops and entries
+    // themselves are read from device memory, uploaded on every call
+    const double nrp[3] = {precision, minLength, maxLength};
     key = fnv(key, P.cmds.data(), sizeof(BCmd) * P.cmds.size());
+    key = fnv(key, &nC, sizeof(nC));
+    key = fnv(key, nrp, sizeof(nrp));
     key = fnv(key, &I->version, sizeof(I->version));
     P.key = key;
     const int nchunks = (I->npat + kChunk - 1) / kChunk;

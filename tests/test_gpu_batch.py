@@ -106,6 +106,25 @@ def test_batched_precision_form_does_not_depend_on_work_item_sizes(case):
     inst.close()
 
 
+def test_batched_replay_takes_the_newton_parameters_of_each_call(case):
+    """The batched pass replays a captured CUDA graph when the plan repeats; a
+    call with another Newton precision must run with it, exactly as a fresh
+    population does."""
+    w, c3s, dls, conn, _ = case
+    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), mixed=True)
+    pop.set_tuning(8, 2)
+    pop.score(c3s, dls, conn, 0.01)
+    again = pop.score(c3s, dls, conn, 1e-4)
+    pop.close()
+    inst.close()
+    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), mixed=True)
+    pop.set_tuning(8, 2)
+    fresh = pop.score(c3s, dls, conn, 1e-4)
+    pop.close()
+    inst.close()
+    assert np.array_equal(again[0], fresh[0]) and np.array_equal(again[1], fresh[1])
+
+
 def test_population_switches_between_batched_and_per_tree_modes(case):
     """One precision-form population: batched (parent tree in FP64 buffers), then
     per-tree (parent rebuilt in ordinary buffers), then batched again."""
