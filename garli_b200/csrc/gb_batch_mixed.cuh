@@ -272,11 +272,12 @@ __device__ __forceinline__ void cp_issue(const View &v, const DevOp &op, int til
             cp16(smem_u32(sl.c), v.tips + (long long)op.c1 * v.npat_pad + (p & ~15));
             cp16(smem_u32(sl.d), v.tips + (long long)op.c2 * v.npat_pad + (p & ~15));
         } else {
+            // the scale exponents only for the lane of category 0 (the one that stores the sum)
             slice(sl.a, op.c1, op.wide & kWideC1);
-            cp16(smem_u32(sl.c), v.scalers + (long long)op.c1 * v.npat_pad + (p & ~3));
+            if (r == 0) cp16(smem_u32(sl.c), v.scalers + (long long)op.c1 * v.npat_pad + (p & ~3));
             if (op.kind == kIntInt) {
                 slice(sl.b, op.c2, op.wide & kWideC2);
-                cp16(smem_u32(sl.d), v.scalers + (long long)op.c2 * v.npat_pad + (p & ~3));
+                if (r == 0) cp16(smem_u32(sl.d), v.scalers + (long long)op.c2 * v.npat_pad + (p & ~3));
             } else {
                 cp16(smem_u32(sl.d), v.tips + (long long)op.c2 * v.npat_pad + (p & ~15));
             }
@@ -327,11 +328,11 @@ __device__ __forceinline__ void cla_tiles_cp(const View &v, const DevOp &op, con
                 pvec_tip(PR, sl.d[p & 15], y);
             } else {
                 slice(sl.a, op.wide & kWideC1, a);
-                m = reinterpret_cast<const int *>(sl.c)[p & 3];
+                if (r == 0) m = reinterpret_cast<const int *>(sl.c)[p & 3];
                 pvec(PL, a, x);
                 if (op.kind == kIntInt) {
                     slice(sl.b, op.wide & kWideC2, b);
-                    m += reinterpret_cast<const int *>(sl.d)[p & 3];
+                    if (r == 0) m += reinterpret_cast<const int *>(sl.d)[p & 3];
                     pvec(PR, b, y);
                 } else {
                     pvec_tip(PR, sl.d[p & 15], y);
