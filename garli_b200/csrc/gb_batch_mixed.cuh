@@ -363,7 +363,7 @@ __device__ __forceinline__ void side_load(const View &v, int b, int tip, bool wi
         return;
     }
     slice_load<R>(v, b, wide, p, r, s.c);
-    s.scale = __ldcg(v.scalers + (long long)b * v.npat_pad + p);
+    if (r == 0) s.scale = __ldcg(v.scalers + (long long)b * v.npat_pad + p);  // only category 0 stores it
 }
 // the side's vector (P_s V_s) (or V_s itself when it has no matrix), FP64
 __device__ __forceinline__ void side_vec(const double c[4], int code, int tip, const double *P, double out[4]) {
