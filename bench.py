@@ -6,25 +6,32 @@ Headline workload (one "step" = one GA generation): 256 candidate trees, each a
 candidate is rescored (its dirty CLAs recomputed, every other CLA shared with
 the base tree) and the three branches at its move's connector are optimised by
 GARLI's Newton-Raphson (nd->left, nd, nd->right), then scored at the optimised
-lengths.
-  * batched precision form (the headline value): all candidates in one
-    persistent kernel launch (FP32 CLAs, FP64 coefficients, sums and Newton);
-  * plain FP64 per-tree path (measured in the same run): GARLI's way, one
-    candidate after another, a host Newton loop per branch.
+lengths.  Three forms run on the same generation in the same process:
+  * batched precision form (the headline value): the whole generation in one
+    CUDA graph (FP32 CLAs, FP64 coefficients, sums and Newton);
+  * plain FP64 batched: the whole generation in one pass with GARLI's FP64
+    arithmetic;
+  * plain FP64 per tree: GARLI's way, one candidate after another, a host
+    Newton loop per branch.
+The ratios of the first to the third (site-updates/s, lnL evaluations/s and
+generation time) are the headline comparison; the second splits it into a
+batching share and a precision share.
 Metric: CLA site-updates per second (pattern x CLA update; the per-step
 partials on the connector count as updates in both forms); lnL evaluations per
 second (edge evaluations: Newton derivative evaluations + final scores) beside it.
-The single-tree step of the 128-taxon x 100,000-site GTR+I+G4 alignment
-(full rescore + all-branch Newton pass) is reported as a secondary object.
+Secondary objects: the 32-taxon x 2,000-site step (full rescore + all-branch
+Newton pass), the 128-taxon x 100,000-site GTR+I+G4 step, and the 20- and
+61-state rescores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times GARLI's CPU path (the oracle restatement, built with
 GARLI's -O3 -ffast-math flags, OpenMP over patterns on all host cores) on a
 bounded sample of the same generation: per candidate the CLAs GARLI would
-recompute after the move, the same three Newton optimisations and the final
-score.  N > 1 runs N independent replicas (one per GPU, no data-path
-collective); value = all replicas' site-updates / max-over-ranks time.
+recompute after the move, the same three Newton optimisations and the score at
+the connector; the engine's library is never loaded in that process.  N > 1
+runs N independent replicas (one per GPU, no data-path collective); value = all
+replicas' site-updates / max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -148,10 +155,21 @@ def profiled_traffic():
         return None
 
 
-def batch_workload(args, seed):
+def batch_workload(args, seed, mathlib=None):
     from garli_b200 import synth
 
-    return synth.batch_workload(seed=seed, ntax=args.batch_ntax, nsites=args.batch_nsites, ncand=args.ncand)
+    return synth.batch_workload(seed=seed, ntax=args.batch_ntax, nsites=args.batch_nsites, ncand=args.ncand,
+                                mathlib=mathlib)
+
+
+def batch_config(args, w, ncand, ws):
+    """The workload's config: identical in both arms (the implementation and its
+    form are reported outside it)."""
+    return {"workload": w.name, "ntax": args.batch_ntax, "nsites": args.batch_nsites, "npat": w.data.npat,
+            "candidates": ncand, "moves": "SPR radius U{1..8} (1 = NNI)", "model": "GTR+G4",
+            "step": "one generation: dirty-CLA rescore + 3-branch Newton + final score per candidate",
+            "newton_precision": args.precision,
+            "l2": "working set > L2 (CLAs 2.3 MB each, coefficients 0.97 GB)", "parallelism": f"replicas{ws}"}
 
 
 def make_workload(args, seed):
@@ -274,7 +292,8 @@ def batch_kernel_roofline(r, args, peak, peak_kind):
     """Achieved bandwidth of the batched pass (one CUDA graph per generation:
     k_level4m per CLA level, k_coef4m per step, k_batch4m for the Newton and
     score runs): its algorithmic bytes over its CUDA-event time on the
-    instance stream (a few extra timed passes)."""
+    instance stream (a few extra timed passes), and the same per phase (every
+    launch bracketed by its own events, launched without the graph)."""
     import torch
 
     w_c3s = r["bw"]
@@ -290,43 +309,60 @@ def batch_kernel_roofline(r, args, peak, peak_kind):
     torch.cuda.synchronize()
     ms = (t1["ms"] - t0["ms"]) / max(1, t1["launches"] - t0["launches"])
     alg = pop.counters()["alg_bytes"]
+    parts = pop.byte_counters()
     achieved = alg / (ms / 1e3) / 1e9
+    # per phase
+    pop.set_phase_timing(True)
+    p0 = pop.phase_timing()
+    for _ in range(n):
+        pop.score(c3s, dls, conn, args.precision)
+    p1 = pop.phase_timing()
+    pop.set_phase_timing(False)
+    kernels = {"levels": "k_level4m", "coefficients": "k_coef4m", "sweeps": "k_batch4m"}
+    phases = {}
+    for k, kname in kernels.items():
+        pms = (p1[k]["ms"] - p0[k]["ms"]) / n
+        nl = (p1[k]["launches"] - p0[k]["launches"]) / n
+        ach = parts[k] / (pms / 1e3) / 1e9 if pms > 0 else None
+        phases[k] = {"kernel": kname, "ms_per_pass": pms, "launches_per_pass": nl,
+                     "algorithmic_bytes_per_pass": parts[k], "achieved": ach,
+                     "frac": (ach / peak) if ach else None}
     traffic = profiled_traffic()
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic.get("bytes_per_pass") if traffic else None,
             "kernel": "batched pass: k_level4m<4> per CLA level, k_coef4m<4> per step, k_batch4m<4> per "
                       "Newton run (one CUDA graph per generation)",
             "peak_kind": f"{peak_kind} hbm_gbs (burst copy)", "ms_per_pass": ms,
-            "algorithmic_bytes_per_pass": alg,
+            "algorithmic_bytes_per_pass": alg, "phases": phases,
             "traffic_note": traffic.get("note") if traffic else "no ncu capture committed"}
 
 
-def e2e_batch(bw, args, device, steps):
-    """The generation through the public call with host buffers: candidate
-    topologies, lengths and connectors go in from pinned host memory, per-candidate
-    lnL / improvement / evaluations and the optimised lengths come back."""
+def e2e_batch(r, args, device, steps, clocks=None):
+    """The generation through the public call with host buffers, on the
+    headline's population right after its timed loop, for as many generations
+    and with the same clock sampler running: candidate topologies, lengths and
+    connectors go in from pinned host memory, per-candidate lnL / improvement /
+    evaluations and the optimised lengths come back; wall-clock time."""
     import torch
 
-    from garli_b200 import engine
-
-    w, c3s, dls, conn = bw
-    inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), device=device, mixed=True)
+    _, c3s, dls, conn = r["bw"]
+    pop = r["pop"]
     pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in (c3s, dls, conn)]
     pop.score(*pin, args.precision)
     torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
     updates = 0
     out = lens = None
-    for _ in range(steps):
-        out, lens = pop.score(*pin, args.precision)
-        updates += pop.counters()["pattern_updates"]
-    torch.cuda.synchronize(device)
-    dt = time.perf_counter() - t0
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            out, lens = pop.score(*pin, args.precision)
+            updates += pop.counters()["pattern_updates"]
+        torch.cuda.synchronize(device)
+        dt = time.perf_counter() - t0
     bi = sum(a.nbytes for a in pin)
     bo = out.nbytes + lens.nbytes
-    pop.close()
-    inst.close()
-    return updates / dt, bi, bo
+    return updates / dt, bi, bo, 1000.0 * dt / steps
 
 
 def single_tree(args, device, rank):
@@ -390,13 +426,15 @@ def nstate_forms(kind, device, reps=3):
     return out
 
 
-def _oracle_candidate(w, c3, dl, X, prec, orc, repeats=1):
+def _oracle_candidate(w, c3, dl, X, prec, orc, model, repeats=1):
     """GARLI's CPU path for one candidate: the tree is built and scored (the
     parent's CLAs), the move's branches are touched so the CLAs GARLI would
     recompute are dirty (SweepDirtynessOverTree), then -- timed -- the rescore,
-    the three Newton optimisations and the final score; ``repeats`` times from
-    the same starting lengths.  Returns (seconds, CLA ops)."""
-    ot = orc.OracleTree(w.data, c3, dl, w.model, fast=True)
+    the three Newton optimisations (nd->left, nd, nd->right) and the score at
+    the optimised lengths (Tree::Score at the connector: only CLAs the
+    optimisation left dirty are recomputed); ``repeats`` times from the same
+    starting lengths.  Returns (seconds, CLA ops)."""
+    ot = orc.OracleTree(w.data, c3, dl, model, fast=True)
     ot.score(0)
     order = [int(c3[X][0]), int(X), int(c3[X][2])]
     tt = 0.0
@@ -409,7 +447,6 @@ def _oracle_candidate(w, c3, dl, X, prec, orc, repeats=1):
         ot.score(0)
         for nd in order:
             ot.optimize_branch(nd, prec)
-        ot.make_all_dirty()
         ot.score(int(X))
         tt += time.perf_counter() - t0
         ops += ot.counts()["cla"] - c0
@@ -417,34 +454,103 @@ def _oracle_candidate(w, c3, dl, X, prec, orc, repeats=1):
     return tt, ops
 
 
+def _oracle_sample(w, c3s, dls, conn, prec, orc, model, cands, repeats, threads):
+    """Candidates ``cands`` of the generation on ``threads`` host threads:
+    (site-updates/s, candidates/s, seconds timed)."""
+    orc.set_threads(threads, fast=True)
+    tt = 0.0
+    ops = 0
+    for i in cands:
+        dt, o = _oracle_candidate(w, c3s[i], dls[i], int(conn[i]), prec, orc, model, repeats=repeats)
+        tt += dt
+        ops += o
+    return ops * w.data.npat / tt, len(cands) * repeats / tt, tt
+
+
 def cpu_baseline(args, bw):
-    """GARLI's CPU path (oracle restatement, GARLI's gcc flags, OpenMP over
-    patterns on all cores) on a bounded sample of the generation."""
+    """GARLI's CPU path (oracle restatement, GARLI's gcc flags) on a bounded
+    sample of the generation: OpenMP over patterns on all host cores (GARLI's
+    --enable-openmp build), and one thread (its default build).  The oracle's
+    model is built with the oracle's own model math."""
     from oracle import oracle as orc
 
     w, c3s, dls, conn = bw
+    model = w.model_with(orc)
     cores = os.cpu_count() or 1
-    orc.set_threads(cores, fast=True)
     k = min(args.cpu_sample_cands, len(conn))
-    tt = 0.0
-    ops = 0
     reps = max(1, args.cpu_repeats)
-    for i in range(k):
-        dt, o = _oracle_candidate(w, c3s[i], dls[i], int(conn[i]), args.precision, orc, repeats=reps)
-        tt += dt
-        ops += o
-    return {"value": ops * w.data.npat / tt, "unit": UNIT, "cores": cores, "kind": "port",
+    v, cps, tt = _oracle_sample(w, c3s, dls, conn, args.precision, orc, model, range(k), reps, cores)
+    k1 = min(4, len(conn))
+    v1, cps1, tt1 = _oracle_sample(w, c3s, dls, conn, args.precision, orc, model, range(k1), 2, 1)
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "candidates_per_s": cps,
             "sample": f"{k} of {len(conn)} candidates x {reps} repeats ({w.data.npat} patterns): dirty-CLA "
-                      f"rescore + 3-branch Newton + final score each, {tt:.1f} s timed"}
+                      f"rescore + 3-branch Newton + score at the connector each, {tt:.1f} s timed",
+            "single_thread": {"value": v1, "unit": UNIT, "cores": 1, "candidates_per_s": cps1,
+                              "sample": f"{k1} candidates x 2 repeats, {tt1:.1f} s timed"}}
+
+
+def config0(args, device, orc_time=True):
+    """SURVEY config 0 as a measured object: 32 taxa x 2,000 sites, GTR+G4,
+    full-tree rescore + one all-branch Newton pass per step, plain FP64 and
+    precision forms (device-timed); GARLI's CPU path on the same step beside
+    them is timed by the caller."""
+    from garli_b200 import synth
+
+    w = synth.dna_small(seed=0)
+    out = {"workload": w.name, "npat": w.data.npat}
+    for name, mixed, steps in (("plain_fp64", False, 20), ("precision", True, 20)):
+        f = run_form(w, args, mixed=mixed, device=device, steps=steps, warmup=3, timing_pass=False)
+        secs = f["ms"] / 1000.0
+        out[name] = {"ms_per_step": f["ms"] / steps, "site_updates_per_s": f["tot"]["pattern_updates"] / secs,
+                     "lnl_evals_per_s": (f["tot"]["scores"] + f["tot"]["edge_evals"]) / secs, "lnl": f["lnl"],
+                     "gpu_launches_per_step": f["launches"] / steps}
+        f["tree"].close()
+        f["inst"].close()
+    return out, w
+
+
+def config0_cpu(args, w):
+    """GARLI's CPU path on the config-0 step (score + all-branch Newton pass)."""
+    from oracle import oracle as orc
+
+    model = w.model_with(orc)
+    res = {}
+    for label, threads in (("all_cores", os.cpu_count() or 1), ("single_thread", 1)):
+        orc.set_threads(threads, fast=True)
+        ot = orc.OracleTree(w.data, w.child3, w.dlen, model, fast=True)
+        ot.score(0)
+        n = 0
+        c0 = ot.counts()
+        t0 = time.perf_counter()
+        while True:
+            for nd in range(1, len(w.dlen)):
+                ot.set_branch_length(nd, float(w.dlen[nd]))
+            ot.make_all_dirty()
+            ot.score(0)
+            ot.optimize_all_branches(args.precision)
+            n += 1
+            if time.perf_counter() - t0 > 2.0:
+                break
+        dt = time.perf_counter() - t0
+        c1 = ot.counts()
+        ot.close()
+        res[label] = {"cores": threads, "ms_per_step": 1000.0 * dt / n,
+                      "site_updates_per_s": (c1["cla"] - c0["cla"]) * w.data.npat / dt,
+                      "lnl_evals_per_s": (c1["derivs"] - c0["derivs"] + n) / dt}
+    return res
 
 
 def reference_arm(args, ws, rank):
+    """GARLI's CPU path on the headline workload.  Nothing of the engine is
+    loaded here: the workload's model is built with the oracle's own model math
+    (the alignment, trees and candidates are the same arrays as the GPU arm's)."""
     if rank != 0:
         return
     from oracle import oracle as orc
 
-    bw = batch_workload(args, seed=4)
+    bw = batch_workload(args, seed=4, mathlib=orc)
     w, c3s, dls, conn = bw
+    model = w.model
     cores = os.cpu_count() or 1
     orc.set_threads(cores, fast=True)
     per = max(1, args.ref_cands_per_step)
@@ -457,7 +563,7 @@ def reference_arm(args, ws, rank):
         for _ in range(per):
             i = nxt % len(conn)
             nxt += 1
-            dt, ops = _oracle_candidate(w, c3s[i], dls[i], int(conn[i]), args.precision, orc)
+            dt, ops = _oracle_candidate(w, c3s[i], dls[i], int(conn[i]), args.precision, orc, model)
             t += dt
             o += ops
         return t, o
@@ -466,22 +572,30 @@ def reference_arm(args, ws, rank):
         step()
     tt = 0.0
     ops = 0
-    for _ in range(max(1, args.steps)):
+    steps = max(1, args.steps)
+    for _ in range(steps):
         dt, o = step()
         tt += dt
         ops += o
     v = ops * w.data.npat / tt
-    steps = max(1, args.steps)
+    k1 = min(2, len(conn))
+    v1, cps1, tt1 = _oracle_sample(w, c3s, dls, conn, args.precision, orc, model, range(k1), 1, 1)
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": args.warmup, "ms_per_step": 1000 * tt / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": w.name, "ntax": args.batch_ntax, "nsites": args.batch_nsites,
-                       "npat": w.data.npat, "candidates": len(conn), "model": "GTR+G4",
-                       "form": "GARLI CPU path, FP64, one candidate at a time", "parallelism": "openmp-patterns"},
+            "config": batch_config(args, w, len(conn), ws),
+            "form": "GARLI CPU path (oracle restatement, GARLI's -O3 -ffast-math flags), FP64, one candidate "
+                    "at a time, OpenMP over patterns",
+            "candidates_per_s": per * steps / tt,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{per} candidate(s) per step (cycling through the generation): dirty-CLA "
-                                       "rescore + 3-branch Newton + final score each"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                                       "rescore + 3-branch Newton + score at the connector each",
+                             "single_thread": {"value": v1, "unit": UNIT, "cores": 1, "candidates_per_s": cps1,
+                                               "sample": f"{k1} candidates, {tt1:.1f} s timed"}},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "site_update_count": "CLA updates GARLI's path performs per candidate (its Newton loop re-dirties "
+                                 "and recomputes CLAs), more than the batched engine's content-keyed plan does "
+                                 "for the same candidates: candidates_per_s compares equal work"}
     print(json.dumps(line), flush=True)
 
 
@@ -535,64 +649,95 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
-    # plain FP64 per-tree path (GARLI's way), same generation
-    plain = run_batch(bw, args, device, mixed=False, sequential=True, steps=max(1, args.steps // 20), warmup=1)
+    # plain FP64 per-tree path (GARLI's way: one candidate after another, host Newton loop)
+    n_plain = max(3, args.steps // 10)
+    plain = run_batch(bw, args, device, mixed=False, sequential=True, steps=n_plain, warmup=1)
+    for k in ("pop", "inst"):
+        plain.pop(k).close()
+    # plain FP64 batched (k_batch4: the whole generation in one pass, GARLI's FP64 arithmetic)
+    n_pb = max(3, args.steps // 4)
+    pbatch = run_batch(bw, args, device, mixed=False, sequential=False, steps=n_pb, warmup=2)
+    for k in ("pop", "inst"):
+        pbatch.pop(k).close()
     # headline: batched precision form
     if pg:
         pg.barrier()
     torch.cuda.synchronize(device)
     clk = ClockSampler(device)
-    mixed = run_batch(bw, args, device, mixed=True, sequential=False, steps=args.steps, warmup=args.warmup,
-                      clocks=clk)
-    torch.cuda.synchronize(device)
-    if pg:
-        pg.barrier()
+    with clk:
+        mixed = run_batch(bw, args, device, mixed=True, sequential=False, steps=args.steps, warmup=args.warmup)
+        torch.cuda.synchronize(device)
+        if pg:
+            pg.barrier()
+        mixed["bw"] = bw
+        # e2e: the same public call from pinned host buffers, same population, as many generations
+        e2e_v, bi, bo, e2e_ms = e2e_batch(mixed, args, device, args.steps)
     from garli_b200.replicas import aggregate
 
-    ms, (updates, edges) = aggregate(pg, mixed["ms"], [mixed["updates"], mixed["edges"]])
+    ms, (updates, edges, e2e_sum) = aggregate(pg, mixed["ms"], [mixed["updates"], mixed["edges"], e2e_v])
     value = updates / (ms / 1000.0)
-    plain_v = plain["updates"] / (plain["ms"] / 1000.0)
-    mixed["bw"] = bw
     roof = batch_kernel_roofline(mixed, args, peak, peak_kind)
-    d0 = float(np.abs(mixed["out"][:, 0] - plain["out"][:, 0]).max())
-    d1 = float(np.abs(mixed["out"][:, 1] - plain["out"][:, 1]).max())
-    dlen = float(np.max(np.abs(mixed["lens"] - plain["lens"]) / np.maximum(plain["lens"], 1e-8)))
+
+    def per_s(r, n):
+        secs = r["ms"] / 1000.0
+        return {"value": r["updates"] / secs, "unit": UNIT, "lnl_evals_per_s": r["edges"] / secs,
+                "ms_per_step": r["ms"] / n, "generations_timed": n}
+
+    mine = per_s(mixed, args.steps)
+    pt = per_s(plain, n_plain)
+    pb = per_s(pbatch, n_pb)
+
+    def diffs(a, b):
+        return {"rescore": float(np.abs(a["out"][:, 0] - b["out"][:, 0]).max()),
+                "optimised": float(np.abs(a["out"][:, 1] - b["out"][:, 1]).max()),
+                "max_rel_dlen": float(np.max(np.abs(a["lens"] - b["lens"]) / np.maximum(b["lens"], 1e-8)))}
+
+    north = {
+        "target": "batched precision form >= 10x the plain FP64 per-tree GPU path, |dlnL| <= 1e-4 per tree",
+        "plain_per_tree": dict(pt, form="plain FP64, one candidate at a time, host Newton loop"),
+        "plain_batched": dict(pb, form="plain FP64, whole generation batched (k_batch4)"),
+        "ratio_site_updates": mine["value"] / pt["value"],
+        "ratio_lnl_evals": mine["lnl_evals_per_s"] / pt["lnl_evals_per_s"],
+        "ratio_generation_time": pt["ms_per_step"] / mine["ms_per_step"],
+        "split_generation_time": {"batching (plain batched vs plain per tree)": pt["ms_per_step"] / pb["ms_per_step"],
+                                  "precision form (batched precision vs plain batched)":
+                                      pb["ms_per_step"] / mine["ms_per_step"]},
+        "max_abs_dlnl_vs_plain_per_tree": diffs(mixed, plain),
+        "max_abs_dlnl_plain_batched_vs_plain_per_tree": diffs(pbatch, plain),
+    }
     tuning = mixed["tuning"]
     cnt = mixed["counters"]
-    for f in (plain, mixed):
-        f["pop"].close()
-        f["inst"].close()
-    e2e_v, bi, bo = e2e_batch(bw, args, device, max(3, args.steps // 4))
-    _, (e2e_v,) = aggregate(pg, 0.0, [e2e_v])
+    launches = mixed["launches"]
+    for k in ("pop", "inst"):
+        mixed.pop(k).close()
+    c0, w0 = (None, None) if args.no_single else config0(args, device)
     single = None if args.no_single else single_tree(args, device, rank)
     nstate = None if args.no_single else {"aa_20_states": nstate_forms("aa", device),
                                           "codon_61_states": nstate_forms("codon", device)}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, bw)
+        if c0 is not None:
+            c0["cpu_oracle"] = config0_cpu(args, w0)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32-cla/f64-coef-sums-newton",
             "data": "synthetic (seeded)",
-            "config": {"workload": w.name, "ntax": args.batch_ntax, "nsites": args.batch_nsites,
-                       "npat": w.data.npat, "candidates": len(conn), "moves": "SPR radius U{1..8} (1 = NNI)",
-                       "model": "GTR+G4", "form": "batched precision (FP32 CLAs, pow2 scalers, FP64 Newton)",
-                       "step": "one generation: dirty-CLA rescore + 3-branch Newton + final score per candidate",
-                       "cla_updates_per_step": cnt["cla_ops"], "l2": "working set > L2 (coefficients 0.97 GB)",
-                       "tuning": tuning, "parallelism": f"replicas{ws}"},
+            "config": batch_config(args, w, len(conn), ws),
+            "form": "batched precision (FP32 CLAs, pow2 scalers, FP64 coefficients, sums and Newton)",
+            "cla_updates_per_step": cnt["cla_ops"], "tuning": tuning,
             "lnl_evals_per_s": edges / (ms / 1000.0),
-            "plain_per_tree": {"value": plain_v, "unit": UNIT, "form": "plain FP64, per candidate, host Newton loop",
-                               "ms_per_step": plain["ms"] / max(1, args.steps // 20),
-                               "lnl_evals_per_s": plain["edges"] / (plain["ms"] / 1000.0)},
-            "mixed_over_plain": (value / ws) / plain_v,
-            "max_abs_dlnl_vs_plain": {"rescore": d0, "optimised": d1, "max_rel_dlen": dlen},
-            "gpu_launches": mixed["launches"],
-            "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+            "candidates_per_s": len(conn) * ws * args.steps / (ms / 1000.0),
+            "north_star": north,
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_sum, "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                    "ms_per_step": e2e_ms, "generations_timed": args.steps},
             "roofline": roof,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "config0": c0,
             "single_tree": single,
             "nstate": nstate,
         }

@@ -121,6 +121,11 @@ struct Instance {
     double tc_corr = kTcCorrUlps;  // mean truncation loss of one UMMA result, in ulps
     double batch_ms = 0.0;  // CUDA-event time of the timed batched launches
     long long batch_timed = 0;
+    // per-phase timing of the batched pass (levels, coefficient passes, Newton /
+    // score runs): every launch bracketed by its own events, no graph
+    bool phase_timing = false;
+    double phase_ms[3] = {0.0, 0.0, 0.0};
+    long long phase_launches[3] = {0, 0, 0};
 
     long long mat_stride() const { return 3LL * R * S * S; }
     long long eig_stride() const { return (long long)S + 2LL * S * S; }
@@ -1669,26 +1674,46 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
     const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
     const int ctiles = (I->npat + kThreads / G - 1) / (kThreads / G);
     const int ncmd = (int)P.cmds.size();
+    // phase timing: events around every launch, by phase (0 levels, 1 coefficient passes, 2 Newton / score)
+    const bool timed = I->phase_timing && !use_graph;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pev;
+    auto mark0 = [&](int phase) {
+        if (!timed) return;
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, I->stream);
+        pev.push_back({phase, {a, b}});
+    };
+    auto mark1 = [&]() {
+        if (timed) cudaEventRecord(pev.back().second.second, I->stream);
+    };
     auto launch_all = [&]() -> cudaError_t {
         cudaError_t e = cudaSuccess;
         for (int l = 0; l < nlev && e == cudaSuccess; l++) {
             const DevOp *ops = I->d_bops + P.cmds[l].a;
             int tpi = tiles;
             void *largs[] = {&v, (void *)&ops, &tpi};
+            mark0(0);
             e = cudaLaunchKernel(lfunc, dim3((ctiles + tiles - 1) / tiles, P.cmds[l].b), dim3(kThreads), largs,
                                  cp_smem_bytes(), I->stream);
+            mark1();
         }
         if (!I->mixed) {
+            mark0(2);
             if (e == cudaSuccess) e = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream);
             if (e == cudaSuccess) e = cudaLaunchKernelExC(&cfg, func, args);
+            mark1();
             return e;
         }
         for (int c = nlev; c < ncmd && e == cudaSuccess;) {
             if (P.cmds[c].type == kBCoef) {
                 int first = P.cmds[c].a, tpi = tiles;
                 void *cargs[] = {&v, &M, &first, &tpi};
+                mark0(1);
                 e = cudaLaunchKernel(coef4m_func(I->R), dim3((ctiles + tiles - 1) / tiles, P.cmds[c].b),
                                      dim3(kThreads), cargs, 0, I->stream);
+                mark1();
                 c++;
                 continue;
             }
@@ -1696,20 +1721,41 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
             while (c1 < ncmd && P.cmds[c1].type != kBCoef) c1++;
             M.cmds = I->d_bcmds + c;
             M.ncmd = c1 - c;
+            mark0(2);
             e = cudaMemsetAsync(I->d_gsync, 0, sizeof(GridSync), I->stream);
             if (e == cudaSuccess) e = cudaLaunchKernelExC(&cfg, func, args);
+            mark1();
             c = c1;
         }
         return e;
+    };
+    auto resolve_phases = [&]() -> int {
+        if (pev.empty()) return GB_SUCCESS;
+        const cudaError_t se = cudaStreamSynchronize(I->stream);
+        for (auto &x : pev) {
+            float ms = 0.f;
+            if (se == cudaSuccess && cudaEventElapsedTime(&ms, x.second.first, x.second.second) == cudaSuccess) {
+                I->phase_ms[x.first] += ms;
+                I->phase_launches[x.first]++;
+            }
+            cudaEventDestroy(x.second.first);
+            cudaEventDestroy(x.second.second);
+        }
+        pev.clear();
+        return se == cudaSuccess ? GB_SUCCESS : GB_ERROR_GENERAL;
     };
     int nkernels = nlev;
     for (int c = nlev; c < ncmd; c++)
         if (!I->mixed ? c == nlev : (P.cmds[c].type == kBCoef || c == nlev || P.cmds[c - 1].type == kBCoef))
             nkernels++;
-    const unsigned long long gkey = P.key ^ ((unsigned long long)tiles << 40) ^ ((unsigned long long)chunks << 48) ^
-                                    ((unsigned long long)rescaleEvery << 56) ^
-                                    (reinterpret_cast<unsigned long long>(I->d_trace) * 0x9E3779B97F4A7C15ULL);
-    if (use_graph && I->use_batch_graph) {
+    // the graph bakes in the work-item sizes, the rescale interval and the trace buffer: all of them key it
+    unsigned long long gkey = P.key;
+    const unsigned long long trace_ptr = reinterpret_cast<unsigned long long>(I->d_trace);
+    gkey = fnv(gkey, &tiles, sizeof(tiles));
+    gkey = fnv(gkey, &chunks, sizeof(chunks));
+    gkey = fnv(gkey, &rescaleEvery, sizeof(rescaleEvery));
+    gkey = fnv(gkey, &trace_ptr, sizeof(trace_ptr));
+    if (use_graph && I->use_batch_graph && !I->phase_timing) {
         if (gkey != I->bgraph_key || !I->bgraph_exec) {
             if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
             if (I->bgraph) cudaGraphDestroy(I->bgraph);
@@ -1742,15 +1788,23 @@ static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int resc
             return GB_SUCCESS;
         }
     }
-    GB_CUDA(launch_all());
+    const cudaError_t le = launch_all();
+    const int prc = resolve_phases();
+    GB_CUDA(le);
     I->launches += nkernels;
-    return GB_SUCCESS;
+    return prc;
 }
 
 // Picks (CLA tiles, edge chunks) per work item by timing whole passes on the
 // real batch.  Every trial starts from the same lengths and matrices (saved
 // and restored on the device); the results do not depend on the choice.
 static int autotune_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery) {
+    struct PhaseOff {  // trial passes are not part of any phase measurement
+        Instance *I;
+        bool was;
+        ~PhaseOff() { I->phase_timing = was; }
+    } phase_off{I, I->phase_timing};
+    I->phase_timing = false;
     const size_t len_bytes = (size_t)I->nmat * sizeof(double);
     const size_t mat_bytes = (size_t)I->nmat * I->mat_stride() * sizeof(double);
     double *save = nullptr;
@@ -1994,7 +2048,7 @@ int gb_batch_newton(int instance, const gb_cla_operation *ops, int opCount, cons
         cudaEventCreate(&te1);
         cudaEventRecord(te0, I->stream);
     }
-    if ((rc = enqueue_batch(I, P, prm, rescaleEvery, tiles, chunks, nC > 0))) {
+    if ((rc = enqueue_batch(I, P, prm, rescaleEvery, tiles, chunks, nC > 0 && !I->phase_timing))) {
         I->rank = rank_before;
         return rc;
     }
@@ -2152,6 +2206,24 @@ int gb_get_batch_timing(int instance, double *out2) {
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
     out2[0] = I->batch_ms;
     out2[1] = (double)I->batch_timed;
+    return GB_SUCCESS;
+}
+
+int gb_set_batch_phase_timing(int instance, int on) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    I->phase_timing = on != 0;
+    return GB_SUCCESS;
+}
+
+int gb_get_batch_phase_timing(int instance, double *out6) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!out6) return GB_ERROR_OUT_OF_RANGE;
+    for (int k = 0; k < 3; k++) {
+        out6[2 * k] = I->phase_ms[k];
+        out6[2 * k + 1] = (double)I->phase_launches[k];
+    }
     return GB_SUCCESS;
 }
 

@@ -4,12 +4,13 @@
 // 4-state data held in caller-owned device arrays, with the same per-site
 // arithmetic as the plain FP64 form's edge kernel (k_edge4 with GARLI's
 // e-based integer scalers).  It exists for callers that cannot call
-// cudaMalloc: code that runs while a CUDA graph is being captured, code
-// inside a host that owns every device allocation through its own pool, or a
-// plugin loaded into such a host, where an allocation would either break the
-// capture or bypass the host's accounting.  The kernel's only scratch -- one
-// (lnL, d1, d2) partial sum per block -- lives in a file-scope __device__
-// array instead of instance memory.
+// cudaMalloc: code inside a host application that owns every device
+// allocation through its own pool (a plugin loaded into such a host), where an
+// allocation would bypass the host's accounting or fail once the pool has
+// reserved the memory, and code on a latency-critical thread, where
+// cudaMalloc's implicit device synchronisation is not allowed.  The kernel's
+// only scratch -- one (lnL, d1, d2) partial sum per block -- lives in a
+// file-scope __device__ array instead of instance memory.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -217,22 +218,30 @@ __global__ void __launch_bounds__(kNaThreads) k_reduce3_static(const double *scr
     }
 }
 
+// Each launch's own result: cudaLaunchKernel returns the error of this launch,
+// so an unrelated error left pending earlier on the thread is neither reported
+// as this call's nor cleared for its owner.
 template <bool D>
-void launch_edge(int R, int nblocks, cudaStream_t st, const EdgeArgs &a, double *scratch) {
+cudaError_t launch_edge(int R, int nblocks, cudaStream_t st, const EdgeArgs &a, double *scratch) {
+    void *f = nullptr;
     switch (R) {
-        case 1: k_edge4_static<1, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        case 2: k_edge4_static<2, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        case 3: k_edge4_static<3, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        case 4: k_edge4_static<4, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        case 5: k_edge4_static<5, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        case 6: k_edge4_static<6, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        case 7: k_edge4_static<7, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
-        default: k_edge4_static<8, D><<<nblocks, kNaThreads, 0, st>>>(a, scratch); break;
+        case 1: f = (void *)k_edge4_static<1, D>; break;
+        case 2: f = (void *)k_edge4_static<2, D>; break;
+        case 3: f = (void *)k_edge4_static<3, D>; break;
+        case 4: f = (void *)k_edge4_static<4, D>; break;
+        case 5: f = (void *)k_edge4_static<5, D>; break;
+        case 6: f = (void *)k_edge4_static<6, D>; break;
+        case 7: f = (void *)k_edge4_static<7, D>; break;
+        default: f = (void *)k_edge4_static<8, D>; break;
     }
+    EdgeArgs args = a;
+    void *kargs[] = {&args, &scratch};
+    return cudaLaunchKernel(f, dim3(nblocks), dim3(kNaThreads), kargs, 0, st);
 }
 
 // Device address of g_edge_scratch, looked up once per device with that
-// device current.  In host code the name g_edge_scratch is only a host-side
+// device current and kept for the life of the process: a cudaDeviceReset on
+// that device invalidates it, and the entry point must not be called after one.  In host code the name g_edge_scratch is only a host-side
 // stand-in for the symbol; handing it to a kernel would fault or, where the
 // GPU can reach host memory, silently use the wrong memory.
 std::mutex g_scratch_mu;
@@ -303,10 +312,14 @@ extern "C" int gb_edge_loglik_static(int resourceNumber, int categoryCount, int 
         a.npat = patternCount;
         const int nblocks = (patternCount + kNaPatternsPerBlock - 1) / kNaPatternsPerBlock;
         cudaStream_t st = static_cast<cudaStream_t>(stream);
-        if (derivatives) launch_edge<true>(categoryCount, nblocks, st, a, scratch);
-        else launch_edge<false>(categoryCount, nblocks, st, a, scratch);
-        k_reduce3_static<<<1, kNaThreads, 0, st>>>(scratch, nblocks, out);
-        const cudaError_t e = cudaGetLastError();
+        cudaError_t e = derivatives ? launch_edge<true>(categoryCount, nblocks, st, a, scratch)
+                                    : launch_edge<false>(categoryCount, nblocks, st, a, scratch);
+        if (e == cudaSuccess) {
+            const double *sc = scratch;
+            int nb = nblocks;
+            void *rargs[] = {(void *)&sc, &nb, &out};
+            e = cudaLaunchKernel((void *)k_reduce3_static, dim3(1), dim3(kNaThreads), rargs, 0, st);
+        }
         if (e != cudaSuccess) rc = fail(GB_ERROR_GENERAL, cudaGetErrorString(e));
     }
     cudaSetDevice(prev);

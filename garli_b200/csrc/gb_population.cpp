@@ -165,6 +165,7 @@ struct Pop {
     std::vector<int> wide_bufs;    // buffers currently marked FP64
     long long c_ops = 0, c_updates = 0, c_evals = 0, c_base_ops = 0, c_edges = 0;
     double c_bytes = 0.0;
+    double c_bytes3[3] = {0.0, 0.0, 0.0};  // of c_bytes: CLA levels, coefficient passes, sweeps
     int npat = 0, ncat = 1;
     std::vector<Key> base_down;  // key of every node's subtree in the base tree (rooted at node 0)
     std::vector<CandNeed> needs; // planning storage, one per candidate (reused)
@@ -528,7 +529,7 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
 
 // Algorithmic device-memory bytes of one batched pass of the precision form
 // (see gbp_get_counters).
-double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps) {
+double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps, double *parts3 = nullptr) {
     // per pattern: a CLA slice is 4R FP32 values and a 4-byte scale exponent
     // (FP64 values for the parent tree's wide buffers), a tip one byte; a
     // step's coefficients are 1 + 3R doubles and a scale exponent; a sweep
@@ -539,14 +540,19 @@ double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps) {
         if (b < p.ntip) return 1.0;
         return (p.base_mode == 1 && !p.wide_bufs.empty() && b < p.base_bufs) ? wide : cla;
     };
-    double per = 0.0;
-    for (const gb_cla_operation &o : P.ops) per += side(o.childClaIndex1) + side(o.childClaIndex2) + cla;
+    double lev = 0.0, cpass = 0.0;
+    for (const gb_cla_operation &o : P.ops) lev += side(o.childClaIndex1) + side(o.childClaIndex2) + cla;
     for (int i = 0; i < 3 * nC; i++) {
         const gb_cla_operation &o = P.step_ops[i];
-        per += coef + side(o.childClaIndex1) + side(o.childClaIndex2) + side(P.steps[i].childIndex);
+        cpass += coef + side(o.childClaIndex1) + side(o.childClaIndex2) + side(P.steps[i].childIndex);
     }
-    per += sweep * (double)sweeps;
-    return per * (double)p.npat;
+    const double sw = sweep * (double)sweeps;
+    if (parts3) {
+        parts3[0] = lev * (double)p.npat;
+        parts3[1] = cpass * (double)p.npat;
+        parts3[2] = sw * (double)p.npat;
+    }
+    return (lev + cpass + sw) * (double)p.npat;
 }
 
 int upload_mats(Pop &p) {
@@ -677,7 +683,7 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
             rc = run_sequential(*p, P, candidateCount, precision, out, lengthsOut);
             p->c_updates = p->c_ops * p->npat;
             p->c_edges = p->c_evals + candidateCount;
-            p->c_bytes = plan_bytes(*p, P, candidateCount, p->c_edges);
+            p->c_bytes = plan_bytes(*p, P, candidateCount, p->c_edges, p->c_bytes3);
         } else {
             rc = gb_batch_newton(p->inst, P.ops.data(), (int)P.ops.size(), P.step_ops.data(),
                                  (int)P.step_ops.size(), P.steps.data(), candidateCount, 3, p->rescaleEvery,
@@ -691,7 +697,7 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
                 p->c_evals = 0;
                 for (int c = 0; c < candidateCount; c++) p->c_evals += (long long)out[4 * c + 3];
                 p->c_edges = p->c_evals + candidateCount;
-                p->c_bytes = plan_bytes(*p, P, candidateCount, p->c_edges);
+                p->c_bytes = plan_bytes(*p, P, candidateCount, p->c_edges, p->c_bytes3);
             }
         }
         if (rc == GB_ERROR_RESCALE_RETRY) {
@@ -714,6 +720,14 @@ int gbp_get_counters(int pop, long long *out6) {
     out6[3] = p->c_base_ops;
     out6[4] = p->c_edges;
     out6[5] = (long long)p->c_bytes;
+    return GB_SUCCESS;
+}
+
+int gbp_get_byte_counters(int pop, double *out3) {
+    Pop *p = get(pop);
+    if (!p) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!out3) return GB_ERROR_OUT_OF_RANGE;
+    for (int k = 0; k < 3; k++) out3[k] = p->c_bytes3[k];
     return GB_SUCCESS;
 }
 

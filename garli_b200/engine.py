@@ -118,6 +118,9 @@ SIGNATURES = {
     "gbp_invalidate": (C.c_int, [C.c_int]),
     "gbp_score_candidates": (C.c_int, [C.c_int, C.c_int, _I, _D, _I, C.c_double, C.c_int, _D, _D]),
     "gbp_get_counters": (C.c_int, [C.c_int, _LL]),
+    "gbp_get_byte_counters": (C.c_int, [C.c_int, _D]),
+    "gb_set_batch_phase_timing": (C.c_int, [C.c_int, C.c_int]),
+    "gb_get_batch_phase_timing": (C.c_int, [C.c_int, _D]),
     "gb_edge_loglik_static": (C.c_int, [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 10 + [C.c_double, C.c_int, C.c_int,
                                                                                           C.c_void_p, C.c_void_p]),
     "gbm_gtr_qmat": (C.c_int, [_D, _D, _D, _D]),
@@ -506,6 +509,22 @@ class Population:
         """Work-item sizes of the batched pass (0, 0: autotune on the next call)."""
         _chk(lib().gb_set_batch_tuning(self.inst.h, int(tiles_per_item), int(chunks_per_item)),
              "gb_set_batch_tuning")
+
+    def byte_counters(self) -> dict:
+        """Algorithmic bytes of the last call by phase."""
+        out = np.zeros(3)
+        _chk(lib().gbp_get_byte_counters(self.h, _p(out, C.c_double)), "gbp_get_byte_counters")
+        return {"levels": float(out[0]), "coefficients": float(out[1]), "sweeps": float(out[2])}
+
+    def set_phase_timing(self, on: bool):
+        _chk(lib().gb_set_batch_phase_timing(self.inst.h, int(on)), "gb_set_batch_phase_timing")
+
+    def phase_timing(self) -> dict:
+        """Accumulated CUDA-event ms and launches per phase of the batched pass."""
+        out = np.zeros(6)
+        _chk(lib().gb_get_batch_phase_timing(self.inst.h, _p(out, C.c_double)), "gb_get_batch_phase_timing")
+        return {k: {"ms": float(out[2 * i]), "launches": int(out[2 * i + 1])}
+                for i, k in enumerate(("levels", "coefficients", "sweeps"))}
 
     def batch_timing(self) -> dict:
         out = np.zeros(2)

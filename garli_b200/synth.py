@@ -120,77 +120,132 @@ def simulate(child3, dlen, model: engine.Model, nsites: int, rng: np.random.Gene
 
 
 @dataclass
+class ModelSpec:
+    """The parameters a synthetic model is drawn with; ``build_model`` turns
+    them into a Model with a chosen library's Q, discrete-gamma and eigen
+    functions (the engine's, or any module with the same five functions), so
+    that each side of a comparison can build the model with its own math."""
+
+    kind: str  # "gtr", "aa" or "codon"
+    pi: np.ndarray
+    exch: np.ndarray | None = None  # GTR: 6 relative rates (last = 1); AA: 190 exchangeabilities
+    alpha: float = 0.5
+    ncat: int = 1
+    pinv: float | None = None
+    kappa: float = 0.0
+    omega: float = 0.0
+
+
+def build_model(spec: ModelSpec, mathlib=None) -> engine.Model:
+    """Model of ``spec`` from ``mathlib``'s gtr_qmat / aa_qmat / codon_qmat,
+    discrete_gamma and eigen (default: the engine's host model math)."""
+    ml = engine if mathlib is None else mathlib
+    if spec.kind == "gtr":
+        Q, bm = ml.gtr_qmat(list(spec.exch), spec.pi)
+    elif spec.kind == "aa":
+        Q, bm = ml.aa_qmat(spec.exch, spec.pi)
+    elif spec.kind == "codon":
+        Q, bm = ml.codon_qmat(spec.kappa, spec.omega, spec.pi)
+    else:
+        raise ValueError(spec.kind)
+    rates = np.asarray(ml.discrete_gamma(spec.alpha, spec.ncat), dtype=np.float64) if spec.ncat > 1 else np.ones(1)
+    ev, U, Ui = ml.eigen(Q, spec.pi)
+    has_pinv = spec.pinv is not None
+    pinv = float(spec.pinv) if has_pinv else 0.0
+    probs = np.full(len(rates), (1.0 - pinv) / len(rates))
+    return engine.Model(spec.pi.shape[0], np.ascontiguousarray(spec.pi, dtype=np.float64), Q, bm, ev, U, Ui,
+                        rates, probs, pinv, has_pinv)
+
+
+@dataclass
 class Workload:
     name: str
     child3: np.ndarray
     dlen: np.ndarray
     model: engine.Model
     data: PatternData
+    spec: ModelSpec | None = None
+
+    def model_with(self, mathlib) -> engine.Model:
+        """The same model built with another library's model math."""
+        return build_model(self.spec, mathlib)
 
 
-def gtr_model(rng, alpha=0.5, ncat=4, pinv=None) -> engine.Model:
+def gtr_spec(rng, alpha=0.5, ncat=4, pinv=None) -> ModelSpec:
     pi = rng.dirichlet([10.0] * 4)
     rel = rng.gamma(2.0, 1.0, size=6)
     rel = rel / rel[5]
-    Q, bm = engine.gtr_qmat(rel[:5].tolist() + [1.0], pi)
-    rates = engine.discrete_gamma(alpha, ncat) if ncat > 1 else np.ones(1)
-    has_pinv = pinv is not None
-    return engine.make_model(4, Q, bm, pi, rates, pinv if has_pinv else 0.0, has_pinv)
+    return ModelSpec("gtr", pi, np.array(rel[:5].tolist() + [1.0]), alpha, ncat if ncat > 1 else 1, pinv)
 
 
-def aa_model(rng, alpha=0.8, ncat=4) -> engine.Model:
+def aa_spec(rng, alpha=0.8, ncat=4) -> ModelSpec:
     exch = rng.gamma(1.0, 1.0, size=190)
     pi = rng.dirichlet([5.0] * 20)
-    Q, bm = engine.aa_qmat(exch, pi)
-    return engine.make_model(20, Q, bm, pi, engine.discrete_gamma(alpha, ncat))
+    return ModelSpec("aa", pi, exch, alpha, ncat)
 
 
-def codon_model(rng) -> engine.Model:
+def codon_spec(rng) -> ModelSpec:
     kappa = rng.uniform(1.5, 4.0)
     omega = rng.uniform(0.1, 1.0)
     pos = [rng.dirichlet([10.0] * 4) for _ in range(3)]
     f = np.array([pos[0][c >> 4] * pos[1][(c >> 2) & 3] * pos[2][c & 3] for c in SENSE_CODONS])
     f = f / f.sum()
-    Q, bm = engine.codon_qmat(kappa, omega, f)
-    return engine.make_model(61, Q, bm, f, np.ones(1))
+    return ModelSpec("codon", f, None, 0.0, 1, None, kappa, omega)
+
+
+def gtr_model(rng, alpha=0.5, ncat=4, pinv=None, mathlib=None) -> engine.Model:
+    return build_model(gtr_spec(rng, alpha, ncat, pinv), mathlib)
+
+
+def aa_model(rng, alpha=0.8, ncat=4, mathlib=None) -> engine.Model:
+    return build_model(aa_spec(rng, alpha, ncat), mathlib)
+
+
+def codon_model(rng, mathlib=None) -> engine.Model:
+    return build_model(codon_spec(rng), mathlib)
 
 
 def dna_to_masks(states: np.ndarray) -> np.ndarray:
     return (1 << states.astype(np.uint8)).astype(np.uint8)
 
 
-def make_dna(ntax, nsites, seed, mean_blen=0.1, alpha=0.5, ncat=4, pinv_range=None, name="dna") -> Workload:
+def make_dna(ntax, nsites, seed, mean_blen=0.1, alpha=0.5, ncat=4, pinv_range=None, name="dna",
+             mathlib=None) -> Workload:
     rng = np.random.default_rng(seed)
     child3, dlen = yule_tree(ntax, rng, mean_blen)
     pinv = float(rng.uniform(*pinv_range)) if pinv_range else None
-    m = gtr_model(rng, alpha, ncat, pinv)
+    spec = gtr_spec(rng, alpha, ncat, pinv)
+    m = build_model(spec, mathlib)
     st = simulate(child3, dlen, m, nsites, rng)
     pd = compress(dna_to_masks(st), 4)
-    return Workload(name, child3, dlen, m, pd)
+    return Workload(name, child3, dlen, m, pd, spec)
 
 
-def dna_small(seed=0) -> Workload:
-    return make_dna(32, 2000, seed, name="dna_gtr_g4_32x2000")
+def dna_small(seed=0, mathlib=None) -> Workload:
+    return make_dna(32, 2000, seed, name="dna_gtr_g4_32x2000", mathlib=mathlib)
 
 
-def dna_large(seed=1, nsites=100_000, ntax=128) -> Workload:
-    return make_dna(ntax, nsites, seed, pinv_range=(0.05, 0.3), name=f"dna_gtr_i_g4_{ntax}x{nsites}")
+def dna_large(seed=1, nsites=100_000, ntax=128, mathlib=None) -> Workload:
+    return make_dna(ntax, nsites, seed, pinv_range=(0.05, 0.3), name=f"dna_gtr_i_g4_{ntax}x{nsites}",
+                    mathlib=mathlib)
 
 
-def aa(seed=2, ntax=64, nsites=20_000) -> Workload:
+def aa(seed=2, ntax=64, nsites=20_000, mathlib=None) -> Workload:
     rng = np.random.default_rng(seed)
     child3, dlen = yule_tree(ntax, rng, 0.15)
-    m = aa_model(rng)
+    spec = aa_spec(rng)
+    m = build_model(spec, mathlib)
     st = simulate(child3, dlen, m, nsites, rng)
-    return Workload(f"aa_g4_{ntax}x{nsites}", child3, dlen, m, compress(st, 20))
+    return Workload(f"aa_g4_{ntax}x{nsites}", child3, dlen, m, compress(st, 20), spec)
 
 
-def codon(seed=3, ntax=32, ncodons=5_000) -> Workload:
+def codon(seed=3, ntax=32, ncodons=5_000, mathlib=None) -> Workload:
     rng = np.random.default_rng(seed)
     child3, dlen = yule_tree(ntax, rng, 0.2)
-    m = codon_model(rng)
+    spec = codon_spec(rng)
+    m = build_model(spec, mathlib)
     st = simulate(child3, dlen, m, ncodons, rng)
-    return Workload(f"codon_gy94_{ntax}x{ncodons}", child3, dlen, m, compress(st, 61))
+    return Workload(f"codon_gy94_{ntax}x{ncodons}", child3, dlen, m, compress(st, 61), spec)
 
 
 # ---------------------------------------------------------------- GA candidates
@@ -316,9 +371,9 @@ def ga_candidates(child3, dlen, count, seed, radius_range=(1, 8)):
     return c3s, dls, conn
 
 
-def batch_workload(seed=4, ntax=64, nsites=50_000, ncand=256):
+def batch_workload(seed=4, ntax=64, nsites=50_000, ncand=256, mathlib=None):
     """The GA-population workload: a Yule base tree, GTR+G4, its alignment, and
     ``ncand`` SPR/NNI candidates of it (radius ~ U{1..8})."""
-    w = make_dna(ntax, nsites, seed, name=f"ga_batch_dna_gtr_g4_{ntax}x{nsites}_{ncand}cand")
+    w = make_dna(ntax, nsites, seed, name=f"ga_batch_dna_gtr_g4_{ntax}x{nsites}_{ncand}cand", mathlib=mathlib)
     c3s, dls, conn = ga_candidates(w.child3, w.dlen, ncand, seed + 1000)
     return w, c3s, dls, conn

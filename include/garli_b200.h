@@ -266,6 +266,13 @@ int gb_get_batch_tuning(int instance, int *out3);
 /* instrumentation (while gb_set_kernel_timing is on): out[0] = CUDA-event ms of
  * the batched pass launches on the instance stream, out[1] = launches timed */
 int gb_get_batch_timing(int instance, double *out2);
+/* instrumentation: with phase timing on, every launch of a batched pass is
+ * bracketed by its own CUDA events and launched directly (no graph);
+ * out[2k] = accumulated ms, out[2k+1] = launches of phase k: 0 = CLA levels,
+ * 1 = coefficient passes, 2 = Newton / score runs.  No counterpart in the
+ * reference (GARLI has no device timing). */
+int gb_set_batch_phase_timing(int instance, int on);
+int gb_get_batch_phase_timing(int instance, double *out6);
 
 /* ---- population layer: a GA generation's candidates on one instance ----
  * A C++ restatement of how GARLI scores the candidates of a generation: each
@@ -300,12 +307,18 @@ int gbp_score_candidates(int pop, int candidateCount, const int *child3s, const 
  * written; 8(1 + 3R) + 12 B per edge-evaluation pattern (at R = 4: 68, 132,
  * 108, 116); [3] base-tree CLA updates since creation */
 int gbp_get_counters(int pop, long long *out6);
+/* the last call's algorithmic device-memory bytes (out6[5]) split by phase:
+ * out[0] CLA levels, out[1] coefficient passes (step partials), out[2] Newton
+ * and score sweeps */
+int gbp_get_byte_counters(int pop, double *out3);
 
 /* ---- edge evaluation without device allocation ----
  * No counterpart in the reference: GARLI's beagle build lets beagle allocate.
- * For callers that cannot call cudaMalloc -- code running while a CUDA graph
- * is captured, or a plugin inside a host that owns every device allocation
- * through its own pool -- this evaluates lnL (and d1, d2) across one branch
+ * For callers that cannot call cudaMalloc -- a plugin inside a host
+ * application that owns every device allocation through its own pool, where an
+ * allocation would bypass the host's accounting or fail once the pool has
+ * reserved the memory, or code on a latency-critical thread that must not take
+ * cudaMalloc's implicit device synchronisation -- this evaluates lnL (and d1, d2) across one branch
  * of 4-state data held entirely in the caller's device arrays, with the plain
  * FP64 form's per-site arithmetic (GARLI's e-based integer scalers).  It
  * allocates nothing: its per-block partial sums live in a fixed 96 KiB array
@@ -323,7 +336,9 @@ int gbp_get_counters(int pop, long long *out6);
  * patternCount above GB_STATIC_EDGE_MAX_PATTERNS is rejected with
  * GB_ERROR_OUT_OF_RANGE.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress): make that first call before any
- * stream capture.  Every call shares the one array, so calls that overlap on
+ * stream capture.  The address is kept until the process exits: a
+ * cudaDeviceReset on that device invalidates it, and the entry point must not
+ * be called after one.  Every call shares the one array, so calls that overlap on
  * the GPU (unordered streams) race; calls ordered on one stream do not. */
 #define GB_STATIC_EDGE_MAX_PATTERNS 4194304
 int gb_edge_loglik_static(int resourceNumber, int categoryCount, int patternCount, const double *partial,

@@ -12,7 +12,8 @@ the model parameters printed by GARLI and GARLI's own score for that tree.
 The GarliScore comments are the pins: GARLI computed them with its CPU path
 before printing the parameters to 5 decimals, so a rescore agrees to about 1e-3.
 
-    python tests/golden/make_fixtures.py [/path/to/garli/trunk]
+    python tests/golden/make_fixtures.py /path/to/garli/trunk
+    GARLI_REFERENCE=/path/containing/garli python tests/golden/make_fixtures.py
 """
 from __future__ import annotations
 
@@ -28,7 +29,12 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from garli_b200 import patterns, treeio  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/garli/trunk"
+if len(sys.argv) > 1:
+    REF = sys.argv[1]
+elif os.environ.get("GARLI_REFERENCE"):
+    REF = os.path.join(os.environ["GARLI_REFERENCE"], "garli", "trunk")
+else:
+    sys.exit("usage: make_fixtures.py /path/to/garli/trunk (or set GARLI_REFERENCE)")
 DATA = os.path.join(REF, "tests", "data")
 
 

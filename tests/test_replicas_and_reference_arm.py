@@ -61,13 +61,40 @@ def test_single_process_aggregate_is_identity():
     assert aggregate(None, 5.0, [1, 2]) == (5.0, [1.0, 2.0])
 
 
+REF_ARGS = ["--steps", "1", "--warmup", "0", "--ref-cands-per-step", "1", "--batch-nsites", "1500", "--ncand", "4"]
+
+
 def test_reference_arm_prints_contract_line():
     env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
-    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0", "--ref-cands-per-step", "1", "--batch-nsites", "1500", "--ncand", "4"],
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference"] + REF_ARGS,
                          capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "site-updates/s"
     assert line["e2e"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "port"
     assert line["higher_is_better"] is True and line["steps"] == 1
+    assert line["cpu_baseline"]["single_thread"]["cores"] == 1
+
+
+def test_reference_arm_loads_no_engine_library_and_shares_the_config():
+    """The reference arm builds its model with the oracle's math: the engine's
+    .so is never mapped in that process, and its config dict is the GPU arm's."""
+    code = (
+        "import sys, json, io, contextlib; sys.argv = ['bench.py', '--impl', 'reference'] + %r\n"
+        "import bench\n"
+        "buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf): bench.main()\n"
+        "line = json.loads(buf.getvalue().strip().splitlines()[-1])\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "from garli_b200 import synth\n"
+        "args = bench.parse()\n"
+        "w = synth.batch_workload(seed=4, ntax=args.batch_ntax, nsites=args.batch_nsites, ncand=args.ncand)[0]\n"
+        "print(json.dumps({'engine_mapped': 'libgarli_b200' in maps, 'oracle_mapped': 'liboracle' in maps,\n"
+        "                  'same_config': line['config'] == json.loads(json.dumps(bench.batch_config(args, w, args.ncand, 1)))}))\n"
+    ) % (REF_ARGS,)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    # the maps are read before the config check builds the workload with the engine's math
+    assert not res["engine_mapped"] and res["oracle_mapped"] and res["same_config"]

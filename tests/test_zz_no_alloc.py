@@ -1,8 +1,9 @@
 """gb_edge_loglik_static, the edge evaluation that allocates no device memory.
 
-Some callers of the engine cannot call cudaMalloc: code that runs while a CUDA
-graph is being captured, and plugins inside a host application that owns every
-device allocation through its own pool.  They evaluate a branch with
+Some callers of the engine cannot call cudaMalloc: plugins inside a host
+application that owns every device allocation through its own pool, and code
+on a latency-critical thread that must not take cudaMalloc's implicit device
+synchronisation.  They evaluate a branch with
 gb_edge_loglik_static on device arrays they already hold; the entry point keeps
 its per-block partial sums in a fixed array inside the library.  Here its lnL,
 d1 and d2 must equal those of the instance path (gb_calculate_edge, reached
