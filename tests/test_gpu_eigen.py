@@ -46,7 +46,7 @@ def test_batched_eigensystems_score_like_the_oracle():
         pytest.fail("no CUDA device visible to the engine")
     w = synth.make_dna(20, 800, seed=5, pinv_range=(0.05, 0.3))
     inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model)
-    ot = orc.OracleTree(w.data, w.child3, w.dlen, w.model)
+    ot = orc.OracleTree(w.data, w.child3, w.dlen, w.model_with(orc))
     m = w.model
     # three models in one launch; slot 0 (the tree's) is replaced by the device result
     rng = np.random.default_rng(3)

@@ -5,7 +5,7 @@ Tolerances:
     entries to 1e-12 (4 states) / 1e-9 (61 states) of each pattern's largest
     entry (P(t) uses the device exp, which may differ from the host's by an
     ulp); integer rescale counts and ranks exactly.
-  * precision form (FP32 CLAs, power-of-two scalers): |dlnL| <= 1e-4 * max(1, npat/2000)
+  * precision form (FP32 CLAs, power-of-two scalers): |dlnL| <= 1e-4
     absolute per tree, derivatives to 1e-4 relative.
 """
 import numpy as np
@@ -26,9 +26,11 @@ def _device():
         pytest.fail("no CUDA device visible to the engine")
 
 
-def _both(pd, c3, dl, model, mixed=False):
+def _both(pd, c3, dl, model, mixed=False, omodel=None):
+    """Engine and oracle on the same tree; ``omodel`` is the same model built
+    with the oracle's own model math (default: ``model`` itself)."""
     inst, tree = engine.tree_engine(pd, c3, dl, model, mixed=mixed)
-    ot = orc.OracleTree(pd, c3, dl, model)
+    ot = orc.OracleTree(pd, c3, dl, model if omodel is None else omodel)
     return inst, tree, ot
 
 
@@ -36,7 +38,7 @@ def _both(pd, c3, dl, model, mixed=False):
 def test_fixture_scores_match_oracle_and_garli(name):
     fx, pd, c3, dl = load_fixture(name)
     m = fixture_model(fx, engine)
-    inst, tree, ot = _both(pd, c3, dl, m)
+    inst, tree, ot = _both(pd, c3, dl, m, omodel=fixture_model(fx, orc))
     lg, lo = tree.score(0), ot.score(0)
     assert abs(lg - lo) <= 1e-8 * abs(lo)
     assert abs(lg - fx["garli_score"]) < 2e-6
@@ -45,7 +47,9 @@ def test_fixture_scores_match_oracle_and_garli(name):
 
 @pytest.mark.parametrize("name", PINS)
 def test_every_cla_and_scaler_matches(name):
-    """After a full score from node 0 every clean CLA equals the oracle's; scalers exactly."""
+    """After a full score from node 0 every clean CLA equals the oracle's; scalers
+    exactly.  Both sides take the same eigensystem here, so the comparison is of
+    the CLA arithmetic alone (the model math is compared in the score tests)."""
     fx, pd, c3, dl = load_fixture(name)
     m = fixture_model(fx, engine)
     inst, tree, ot = _both(pd, c3, dl, m)
@@ -74,6 +78,8 @@ def test_every_cla_and_scaler_matches(name):
 
 @pytest.mark.parametrize("name", PINS)
 def test_branch_derivatives(name):
+    """d1 near an optimum is a small sum of large terms of both signs: the same
+    eigensystem on both sides keeps the comparison to the derivative arithmetic."""
     fx, pd, c3, dl = load_fixture(name)
     m = fixture_model(fx, engine)
     inst, tree, ot = _both(pd, c3, dl, m)
@@ -88,7 +94,7 @@ def test_branch_derivatives(name):
 def test_root_choice_and_rescale_invariance():
     fx, pd, c3, dl = load_fixture(PINS[0])
     m = fixture_model(fx, engine)
-    inst, tree, ot = _both(pd, c3, dl, m)
+    inst, tree, ot = _both(pd, c3, dl, m, omodel=fixture_model(fx, orc))
     ref = ot.score(0)
     for nd in [0] + list(range(pd.ntax + 1, c3.shape[0])):
         tree.make_all_dirty()
@@ -101,7 +107,7 @@ def test_root_choice_and_rescale_invariance():
 def test_config0_score_and_newton_pass():
     """32 taxa x 2,000 sites GTR+G4: full score plus one all-branch Newton pass."""
     w = synth.dna_small()
-    inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model)
+    inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model, omodel=w.model_with(orc))
     lg, lo = tree.score(0), ot.score(0)
     assert abs(lg - lo) <= 1e-8 * abs(lo)
     ig, fg = tree.optimize_all_branches(0.01)
@@ -145,7 +151,7 @@ def test_rescale_retry_path_matches_oracle():
 @pytest.mark.parametrize("kind", ["aa", "codon"])
 def test_nstate_synthetic(kind):
     w = synth.aa(seed=4, ntax=16, nsites=600) if kind == "aa" else synth.codon(seed=5, ntax=12, ncodons=300)
-    inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model)
+    inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model, omodel=w.model_with(orc))
     lg, lo = tree.score(0), ot.score(0)
     assert abs(lg - lo) <= 1e-8 * abs(lo)
     for nd in (1, 5, w.data.ntax + 2):
@@ -158,12 +164,12 @@ def test_mixed_precision_form(name):
     fx, pd, c3, dl = load_fixture(name)
     m = fixture_model(fx, engine)
     inst, tree = engine.tree_engine(pd, c3, dl, m, mixed=True)
-    ot = orc.OracleTree(pd, c3, dl, m)
+    ot = orc.OracleTree(pd, c3, dl, fixture_model(fx, orc))
     lg, lo = tree.score(0), ot.score(0)
-    assert abs(lg - lo) <= 1e-4 * max(1.0, pd.npat / 2000)
+    assert abs(lg - lo) <= 1e-4
     for nd in (1, 4, pd.ntax + 3):
         g, o = tree.derivatives(nd), ot.derivatives(nd)
-        assert abs(g[0] - o[0]) <= 1e-4 * max(1.0, pd.npat / 2000)
+        assert abs(g[0] - o[0]) <= 1e-4
         assert abs(g[1] - o[1]) <= 1e-4 * max(1.0, abs(o[1]))
         assert abs(g[2] - o[2]) <= 1e-4 * max(1.0, abs(o[2]))
 
@@ -233,12 +239,12 @@ def test_device_newton_pass_equals_host_pass(mixed):
     if mixed:
         bl, lnl, imp = res["persistent"]
         assert np.allclose(bl, res["host"][0], rtol=1e-3, atol=1e-8)
-        assert abs(lnl - res["host"][1]) <= 1e-4 * max(1.0, w.data.npat / 2000)
+        assert abs(lnl - res["host"][1]) <= 1e-4
 
 
 def test_device_newton_pass_matches_oracle_and_is_repeatable():
     w = synth.make_dna(48, 2500, seed=22)
-    inst, tree, ot = _both(w.data, w.child3, w.dlen * 0.7, w.model)
+    inst, tree, ot = _both(w.data, w.child3, w.dlen * 0.7, w.model, omodel=w.model_with(orc))
     for _ in range(2):  # second pass replays the cached graph from a different start
         tree.score(0)
         ot.score(0)

@@ -9,7 +9,7 @@ Tolerances: every CLA entry within 2e-5 of its pattern's largest entry against
 the CUDA-core kernel, median over patterns within 1e-6 (FP32-level agreement
 that grows with the depth of the CLA: both paths round every level to FP32
 independently); integer scalers identical;
-lnL, d1, d2 as the precision form's bar: |dlnL| <= 1e-4 * max(1, npat/2000)
+lnL, d1, d2 as the precision form's bar: |dlnL| <= 1e-4
 absolute, derivatives 1e-4 relative to max(1, |d|).
 """
 import numpy as np
@@ -57,8 +57,8 @@ def test_tensor_core_clas_match_cuda_core_clas(kind):
 def test_tensor_core_precision_form_matches_oracle(kind):
     w = _workload(kind)
     inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model, mixed=True)
-    ot = orc.OracleTree(w.data, w.child3, w.dlen, w.model)
-    tol = 1e-4 * max(1.0, w.data.npat / 2000)
+    ot = orc.OracleTree(w.data, w.child3, w.dlen, w.model_with(orc))
+    tol = 1e-4
     lg, lo = tree.score(0), ot.score(0)
     assert abs(lg - lo) <= tol, (lg, lo)
     for nd in (1, 3, w.data.ntax + 2):
