@@ -118,7 +118,6 @@ struct Instance {
     unsigned long long bgraph_key = 0;
     int use_batch_graph = 1;
     int use_tc = 1;  // precision form, 20 / 61 states: CLA updates on the tensor cores
-    double tc_corr = kTcCorrUlps;  // mean truncation loss of one UMMA result, in ulps
     double batch_ms = 0.0;  // CUDA-event time of the timed batched launches
     long long batch_timed = 0;
     // per-phase timing of the batched pass (levels, coefficient passes, Newton /
@@ -242,29 +241,29 @@ static int ns_edge_tile(const Instance *I, size_t *smem) {
     return tp;
 }
 
-// tensor-core CLA update (gb_tc.cuh): supported shapes and launch parameters
+// tensor-core CLA update (gb_tc.cuh): supported shapes and launch parameters.
+// 20 states with up to 4 categories, 61 states with one (the FP32 tiles of
+// both children, the digit planes and the output tile must fit one CTA).
 static bool tc_supported(const Instance *I) {
-    return I->mixed && I->use_tc && ((I->S == 20 && I->R <= 8) || (I->S == 61 && I->R <= 2));
-}
-template <int S, int R>
-static size_t tc_smem_bytes() {
-    // at most 512 / COLS CTAs may share an SM's TMEM: shared memory is sized so
-    // that no more fit (an allocation would otherwise wait for a finishing CTA)
-    const int maxc = 512 / TcSmem<S, R>::COLS;
-    const size_t floor_b = 233472 / (maxc + 1) + 1024;
-    return std::min<size_t>(232448, std::max<size_t>(TcSmem<S, R>::BYTES, floor_b));
+    return I->mixed && I->use_tc && ((I->S == 20 && I->R <= 4) || (I->S == 61 && I->R == 1));
 }
 static void *tc_func(int S, int R, size_t *smem) {
-#define GB_TC(s, r)                       \
-    if (S == s && R == r) {               \
-        *smem = tc_smem_bytes<s, r>();    \
-        return (void *)k_cla_tc<s, r>;    \
+#define GB_TC(s, r)                                  \
+    if (S == s && R == r) {                          \
+        *smem = I8Cfg<s, r>::BYTES;                  \
+        return (void *)k_cla_i8<s, r>;               \
     }
-    GB_TC(20, 1) GB_TC(20, 2) GB_TC(20, 3) GB_TC(20, 4) GB_TC(20, 5) GB_TC(20, 6) GB_TC(20, 7) GB_TC(20, 8)
-    GB_TC(61, 1) GB_TC(61, 2)
+    GB_TC(20, 1) GB_TC(20, 2) GB_TC(20, 3) GB_TC(20, 4) GB_TC(61, 1)
 #undef GB_TC
     *smem = 0;
     return nullptr;
+}
+// grid of a tensor-core level launch: tiles per op split so that the level
+// fills the SMs about twice over (one CTA per SM at a time; each CTA runs a
+// pipeline over its tiles of one op)
+static dim3 tc_grid(const Instance *I, int ntiles, int nops) {
+    const int want = (2 * I->nsm + nops - 1) / nops;
+    return dim3(std::max(1, std::min(ntiles, want)), nops);
 }
 
 static int set_smem_attrs() {
@@ -272,7 +271,7 @@ static int set_smem_attrs() {
     GB_CUDA(cudaFuncSetAttribute(k_eigen_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)eigen_smem_bytes(61)));
     for (int S : {20, 61})
-        for (int R = 1; R <= 8; R++) {
+        for (int R = 1; R <= 4; R++) {
             size_t sm = 0;
             void *f = tc_func(S, R, &sm);
             if (f) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -349,13 +348,12 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
                 if (I->mixed) k_cla_ns<false><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
                 else k_cla_ns<true><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
             }
-            const int first = I->kpad / kTcM, nt = I->npat_pad / kTcM - first;
+            int first = I->kpad / kTcM, nt = I->npat_pad / kTcM - first;
             if (tc && nt > 0) {
                 size_t tsm = 0;
                 void *f = tc_func(I->S, I->R, &tsm);
-                double corr = I->tc_corr;
-                void *args[] = {&v, &L, (void *)&first, &corr};
-                GB_CUDA(cudaLaunchKernel(f, dim3(nt, L.n), dim3(kTcThreads), args, tsm, I->stream));
+                void *args[] = {&v, &L, (void *)&first, (void *)&nt};
+                GB_CUDA(cudaLaunchKernel(f, tc_grid(I, nt, L.n), dim3(kTcThreads), args, tsm, I->stream));
             }
         }
         int rc = check_launch(I);
@@ -928,6 +926,22 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
     out[0] = I->h_result[0];
     out[1] = D ? I->h_result[1] : 0.0;
     out[2] = D ? I->h_result[2] : 0.0;
+    if (*I->h_status & kStatusTcRange) {
+        // a product maximum below the tensor-core path's range: the CLAs are
+        // recomputed on the CUDA cores (the tree drivers redo the score on
+        // GB_ERROR_RESCALE_RETRY; the precision form's scaling ignores rescaleEvery)
+        I->use_tc = 0;
+        I->graph_key = 0;
+        GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        return GB_ERROR_RESCALE_RETRY;
+    }
+    if (*I->h_status & kStatusTcTimeout) {
+        GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        g_last_error = "tensor-core CLA update: an mbarrier wait exceeded its bound";
+        return GB_ERROR_GENERAL;
+    }
     if (*I->h_status & kStatusRescaleRetry) {
         GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
         GB_CUDA(cudaStreamSynchronize(I->stream));
@@ -1206,13 +1220,13 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                                    dim3((ns_pat + ns_tp - 1) / ns_tp, L.n), ns_smem, args);
                     }
                     int first = I->kpad / kTcM;
-                    const int nt = I->npat_pad / kTcM - first;
+                    int nt = I->npat_pad / kTcM - first;
                     if (!rc && tc && nt > 0) {
                         size_t tsm = 0;
                         void *f = tc_func(I->S, I->R, &tsm);
-                        void *args[] = {&v, &L, &first, &I->tc_corr};
+                        void *args[] = {&v, &L, &first, &nt};
                         B.block = dim3(kTcThreads);
-                        rc = B.add(B.g, &prev, f, dim3(nt, L.n), tsm, args);
+                        rc = B.add(B.g, &prev, f, tc_grid(I, nt, L.n), tsm, args);
                         B.block = dim3(kThreads);
                     }
                 }
@@ -2189,15 +2203,6 @@ int gb_set_buffer_precision(int instance, int bufferIndex, int fp64) {
         I->wide[b + 1] = 0;
     }
     I->version++;
-    return GB_SUCCESS;
-}
-
-int gb_set_tensor_core_correction(int instance, double ulps) {
-    Instance *I = get(instance);
-    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
-    if (!(ulps >= 0.0 && ulps <= 8.0)) return GB_ERROR_OUT_OF_RANGE;
-    I->tc_corr = ulps;
-    I->graph_key = 0;
     return GB_SUCCESS;
 }
 

@@ -1,331 +1,556 @@
 // gb_tc.cuh -- tensor-core CLA update for the 20- and 61-state models
-// (precision form, FP32 CLA segment).
+// (precision form, FP32 CLA segment), with exact integer accumulation.
 //
 // Per rate category r the update is two dense products followed by an
 // element-wise one (Tree::CalcFullCLAInternalInternalNState, tree.cpp:7843):
 //     dest[p, r, i] = (sum_j P1_r[i][j] L[p, r, j]) * (sum_j P2_r[i][j] R[p, r, j]).
-// A CTA takes 128 patterns of one op, one child at a time with as many rate
-// categories per round as TMEM holds.  Each product is a 128 x 32 x K UMMA
-// per 32-state half (M = patterns, K = states padded to 24 / 64) issued by one
-// thread with tcgen05.mma kind::tf32, operands in shared memory (K-major, no
-// swizzle), results in TMEM.  Operands are split x = hi + lo with hi = tf32(x),
-// lo = tf32(x - hi) (3xTF32): A.B ~ Ahi.Bhi + Ahi.Blo + Alo.Bhi.  The tensor
-// core's FP32 accumulation truncates, so the dominant Ahi.Bhi term is never
-// accumulated across instructions: every 8-wide K step writes its own TMEM
-// region, the regions are summed in FP64 on the CUDA cores, each plus the
-// measured mean truncation loss of one instruction (corr_ulps ulp of its
-// result) unless the row is exact (a one-hot tip); only the small cross terms
-// share an accumulator.  A tip child
-// is a one-hot row (all ones when missing), so every op kind is the same
-// product.  Products of the two children are kept per pattern in FP64 shared
-// memory; the pattern's power-of-two normalisation over all categories and
-// states follows, and FP32 stores use unbiased stochastic rounding.
-// Every mbarrier wait is bounded; a CTA always frees its TMEM.
+//
+// Each product runs on the tensor cores as signed 8-bit digit products with
+// 32-bit integer accumulation (tcgen05.mma kind::i8), which is exact: nothing
+// is rounded or truncated inside the tensor core.  The operands are split into
+// base-256 digits over a per-row power-of-two scale (the scheme of Ootomo,
+// Ozaki and Yokota, "DGEMM on integer matrix multiplication unit", 2024):
+//   * a child CLA row (pattern p, category r) with max_j L < 2^eA is held as
+//     the 38-bit integer round(L 2^(38-eA)): |L - Lq| <= 2^(eA-39);
+//   * a row i of P_r with max_j P < 2^eB as round(P 2^(38-eB)):
+//     |P - Pq| <= 2^(eB-39);
+//   * each integer N is written with five balanced digits d_0..d_4 in
+//     [-128, 127] (d_0 most significant): the bytes of N + 0x8080808080, each
+//     less 128;
+//   * the digit products d_k . e_l with k + l = w are summed into class w
+//     (w = 0..4, fifteen products), and the classes are combined in 64-bit
+//     integers:  sum_j Pq Lq ~ 2^(eA+eB-44) (C0 2^32 + C1 2^24 + C2 2^16 + C3 2^8 + C4).
+//     The dropped classes (k + l >= 5) are sums of products of low-order
+//     balanced digits, of either sign: their error has no bias.
+// Error bound of one product, absolute, with P's rows summing to at most 1
+// (2^eA <= 2 max_j L, 2^eB <= 2):
+//     |sum_j P L - computed| <= (2^-38 + 2^-38 S + 2^-34 S) max_j L,
+// the terms from L's and P's representation and from the dropped classes:
+// 1.2e-9 max_j L for 20 states, 3.7e-9 for 61; the 64-bit sum is converted to
+// FP64 once (relative 2^-53).  That is below the FP32 storage of the result
+// (relative 2^-24, unbiased stochastic rounding), which stays the dominant
+// error of the precision form.  Tip children are not put on the tensor cores:
+// their product is a column of P (or a row sum, for missing data) read in FP64.
+//
+// One CTA per SM (about 200 KB of shared memory) and warp roles:
+//   warps 0-3  epilogue: read the class sums back from TMEM (tcgen05.ld),
+//              combine, multiply the two children, round stochastically to
+//              FP32 into a shared tile; per pattern the power-of-two
+//              normalisation and the integer scaler; coalesced stores;
+//   warps 4-7  producer: 1-D bulk copies (cp.async.bulk, this GPU's own
+//              memory, no multicast) of both children's FP32 tiles into
+//              shared memory, row exponents, digit planes in the UMMA
+//              K-major layout;
+//   warp 8     one thread issues the UMMAs (M = 128 patterns, N = 32 states,
+//              K = 32 digits) into a ring of three TMEM regions (5 classes x
+//              32 columns each) and commits them to mbarriers.
+// Every wait is bounded; a timeout sets a status bit, the roles wind down,
+// copies and MMAs in flight are waited for (bounded) and TMEM is freed.
+// A pattern whose product maximum is below 2^-64 (FP32 would lose digits of
+// its smaller entries) sets kStatusTcRange; the engine then recomputes the
+// CLAs on the CUDA cores.
 #pragma once
 #include "gb_batch_mixed.cuh"
 #include "gb_common.cuh"
+#include "gb_stage.cuh"
 
 namespace gb {
 
-enum : int { kStatusTcTimeout = 8 };
-// mean loss, in ulps of the result, of one tcgen05.mma kind::tf32 result with
-// FP32 accumulation (truncating alignment and normalisation), added back to
-// every inexact K-step result.  Measured on B200: the lnL bias against the
-// FP64 oracle is linear in this value and crosses zero at 0.63-0.70 ulp on the
-// 20- and 61-state test and benchmark alignments (0 ulp: -4e-8 relative lnL;
-// no correction of the accumulated form: -1.2e-7).
-constexpr double kTcCorrUlps = 0.66;
-constexpr int kTcM = 128;      // patterns per CTA (UMMA M)
-constexpr int kTcThreads = 256;  // two warpgroups: both stage; each reads back half of the TMEM columns
+enum : int { kStatusTcTimeout = 8, kStatusTcRange = 16 };
+constexpr int kTcM = 128;                       // patterns per tile (UMMA M)
+constexpr int kTcEpiWarps = 4, kTcProdWarps = 4;
+constexpr int kTcThreads = 32 * (kTcEpiWarps + kTcProdWarps + 1);
+constexpr int kDigA = 5, kDigB = 5, kTcClasses = 5;
+constexpr unsigned long long kDigBias = 0x8080808080ULL;  // + 128 in every digit position
+constexpr int kTcRegions = 3, kTcRegionCols = kTcClasses * 32;
+constexpr int kTcSlots = 2;
+constexpr int kBarEpi = 1, kBarProd = 2;        // named barriers (0 is __syncthreads)
 
-template <int S>
-struct TcShape {
-    static constexpr int KP = (S + 7) / 8 * 8;     // K padded to the tf32 UMMA K step (8)
-    static constexpr int NP = (S + 15) / 16 * 16;  // N padded to a multiple of 16
+// Shapes and shared-memory layout of one CTA.  K (the "to" state j) is padded
+// to whole 32-digit UMMA K steps, N (the "from" state i) to 32-state halves.
+template <int S, int R>
+struct I8Cfg {
+    static constexpr int KB = (S + 31) / 32 * 32;  // digit bytes per row
+    static constexpr int KSTEPS = KB / 32;
+    static constexpr int NH = (S + 31) / 32;
+    static constexpr int NPAD = NH * 32;
+    static constexpr int RS = R * S;
+    static constexpr int RSP = RS | 1;              // odd row stride of the output tile: no bank conflicts
+    static constexpr int STAGE = kTcM * RS * 4;     // FP32 tile of one child
+    static constexpr int APLANE = kTcM * KB;
+    static constexpr int ASLOT = kDigA * APLANE;    // digits of one (child, category)
+    static constexpr int BPLANE = NPAD * KB;
+    static constexpr int BSET = kDigB * BPLANE;     // digits of one P_r
+    static constexpr int SBO = KB * 8;              // bytes between 8-row core-matrix groups
+    static constexpr int OFF_STAGE = 0;
+    static constexpr int OFF_ASLOT = OFF_STAGE + 2 * STAGE;
+    static constexpr int OFF_B = OFF_ASLOT + kTcSlots * ASLOT;
+    static constexpr int OFF_OUT = OFF_B + 2 * R * BSET;
+    static constexpr int OFF_SB = OFF_OUT + kTcM * RSP * 4;     // double [2][R][NPAD]: 2^(eB - 22)
+    static constexpr int OFF_TSUM = OFF_SB + 2 * R * NPAD * 8;  // double [2][R][NPAD]: row sums of P
+    static constexpr int OFF_EA = OFF_TSUM + 2 * R * NPAD * 8;  // int [2 tiles][2 children][R][128]
+    static constexpr int OFF_ROW = OFF_EA + 2 * 2 * R * kTcM * 4;  // float [128]: 2^-e of each pattern
+    static constexpr int BYTES = OFF_ROW + kTcM * 4;
+    static_assert(STAGE % 16 == 0 && OFF_ASLOT % 16 == 0 && OFF_B % 16 == 0, "bulk-copy / UMMA alignment");
 };
 
-__device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+// byte offset of digit (row n, byte k) of a K-major operand with KB bytes
+// per row in the canonical no-swizzle layout: 8-row x 16-byte core matrices,
+// K-adjacent ones 128 B apart (LBO), 8-row groups KB * 8 B apart (SBO)
+__device__ __forceinline__ uint32_t i8_off(int n, int k, int KB) {
+    return (uint32_t)(((n >> 3) * (KB >> 4) + (k >> 4)) * 128 + (n & 7) * 16 + (k & 15));
 }
 
-// byte offset of element (row m, column k) of a K-major operand with KP
-// columns in the canonical no-swizzle layout: 8-row x 16-byte core matrices,
-// the K-adjacent core matrices 128 B apart (LBO), 8-row groups KP*32 B apart (SBO)
-__device__ __forceinline__ uint32_t kmaj_off(int m, int k, int KP) {
-    return (uint32_t)(((m >> 3) * (KP >> 2) + (k >> 2)) * 128 + (m & 7) * 16 + (k & 3) * 4);
-}
-
-// UMMA shared-memory descriptor: start address, LBO, SBO (all >> 4), version 1,
-// base offset 0, no swizzle
+// UMMA shared-memory descriptor: start address, LBO, SBO (all >> 4),
+// descriptor version 1 (bit 46), base offset 0, no swizzle
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
            ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ULL << 46);
 }
 
-// instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N
-__host__ __device__ constexpr uint32_t tc_idesc(int N) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
-}
+// instruction descriptor of kind::i8: D = S32 (bits 4-5 = 2), A = B = signed
+// 8-bit (format 1, bits 7-9 and 10-12), both K-major, N = 32, M = 128
+constexpr uint32_t kI8Idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
 
-__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+__device__ __forceinline__ void umma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(kI8Idesc), "r"(acc));
 }
-
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, float v[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = __uint_as_float(r[j]);
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
 }
-
-__device__ __forceinline__ void tc_ld8_nw(uint32_t taddr, uint32_t r[8]) {
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t r[8]) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr));
 }
-__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+// 1-D bulk copy global -> shared of this CTA, completion counted on mbar
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(mbar)
+        : "memory");
+}
+// named barrier over `n` threads that also agrees on a flag: true only if
+// every participant passed true (a role whose wait gave up leaves together)
+__device__ __forceinline__ bool group_all(bool ok, int id, int n) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)ok), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
+}
 
-// Stage rows [p0, p0 + 128) of one child (CLA or tip) for category r as hi/lo
-// tf32 operands, four K-consecutive elements (one 16-byte core-matrix row
-// segment) per step; the global loads are float4 when rows are 16-byte aligned.
-template <int S, int R>
-__device__ __forceinline__ void tc_stage_a(const View &v, int child, bool tip, int p0, int r, unsigned char *hi,
-                                           unsigned char *lo) {
-    constexpr int KP = TcShape<S>::KP, KQ = KP / 4;
-    constexpr bool VEC = (R * S) % 4 == 0 && S % 4 == 0;
-    const float *src = tip ? nullptr : cla_ptr<float>(v, child, p0, R * S);
-#pragma unroll 2
-    for (int idx = threadIdx.x; idx < kTcM * KQ; idx += blockDim.x) {
-        const int m = idx / KQ, k0 = (idx % KQ) * 4;
-        const int p = p0 + m;
-        float x[4] = {0.f, 0.f, 0.f, 0.f};
-        if (p < v.npat) {
-            if (tip) {
-                const int code = v.tips[(long long)child * v.npat_pad + p];
-#pragma unroll
-                for (int j = 0; j < 4; j++) x[j] = (k0 + j < S && (code >= S || code == k0 + j)) ? 1.f : 0.f;
-            } else if (VEC && k0 + 4 <= S) {
-                const float4 q = __ldg(reinterpret_cast<const float4 *>(src + (long long)m * R * S + r * S + k0));
-                x[0] = q.x;
-                x[1] = q.y;
-                x[2] = q.z;
-                x[3] = q.w;
-            } else {
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    if (k0 + j < S) x[j] = __ldg(src + (long long)m * R * S + r * S + k0 + j);
-            }
+// bounded wait that also gives up as soon as another role has given up
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile int *abort) {
+    unsigned long long t0 = 0;
+    for (long long it = 0; it < (1LL << 24); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 255) == 0) {
+            if (*abort) return false;
+            const unsigned long long t = stage_ns();
+            if (it == 0) t0 = t;
+            else if (t - t0 > 2000000000ULL) break;
         }
-        float h[4], l[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            h[j] = to_tf32(x[j]);
-            l[j] = to_tf32(x[j] - h[j]);
-        }
-        const uint32_t off = kmaj_off(m, k0, KP);
-        *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
     }
+    *abort = 1;
+    return false;
 }
 
-// Stage P_r (rows = "from" states i as N, columns = "to" states j as K).
-template <int S, int R>
-__device__ __forceinline__ void tc_stage_b(const View &v, int mat, int r, unsigned char *hi, unsigned char *lo) {
-    constexpr int KP = TcShape<S>::KP, NP = TcShape<S>::NP, KQ = KP / 4;
-    const double *P = v.mats + (long long)mat * v.mat_stride + (long long)r * S * S;
-    for (int idx = threadIdx.x; idx < NP * KQ; idx += blockDim.x) {
-        const int n = idx / KQ, k0 = (idx % KQ) * 4;
-        float h[4], l[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const float x = (n < S && k0 + j < S) ? (float)__ldg(P + n * S + k0 + j) : 0.f;
-            h[j] = to_tf32(x);
-            l[j] = to_tf32(x - h[j]);
-        }
-        const uint32_t off = kmaj_off(n, k0, KP);
-        *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-    }
+// 38-bit fixed point of a non-negative float over 2^eA (value < 2^eA):
+// round(x 2^(38 - eA)), from the float's bits (exact shifts, round half up);
+// below 2^(eA-39) it is 0
+__device__ __forceinline__ unsigned long long fix38(uint32_t bits, int eA) {
+    const int e = (int)((bits >> 23) & 0xff);
+    if (e == 0) return 0ull;  // zero or subnormal (< 2^-126): far below any row scale in use
+    const uint32_t m = (bits & 0x7fffffu) | 0x800000u;  // value = m 2^(e - 150)
+    const int sh = e - 112 - eA;                         // N = m 2^sh, sh <= 14: N < 2^38
+    if (sh >= 0) return (unsigned long long)m << sh;
+    const int s = -sh;
+    if (s > 25) return 0ull;
+    return (unsigned long long)((m + (1u << (s - 1))) >> s);
+}
+
+// exponent eA with max < 2^eA for a row maximum's bits (0 for an all-zero row)
+__device__ __forceinline__ int row_exp(uint32_t maxbits) {
+    const int e = (int)((maxbits >> 23) & 0xff);
+    return e == 0 ? 0 : e - 126;
 }
 
 template <int S, int R>
-struct TcSmem {
-    static constexpr int KP = TcShape<S>::KP, NP = TcShape<S>::NP;
-    static constexpr int KB = KP / 8;            // K steps
-    static constexpr int NH = NP / 32;           // 32-state halves of N
-    static constexpr int RCOLS = (KB + 1) * 32;  // TMEM columns of one (category, half): K-step regions + cross terms
-    static constexpr int A_BYTES = kTcM * KP * 4, B_BYTES = NP * KP * 4;
-    static constexpr int RSP = R * S + 1;  // product row stride (odd: no bank conflicts between rows)
-    static constexpr int PROD_BYTES = kTcM * RSP * 8;
-    // categories per round.  Measured on B200 (20 states, 4 categories): one
-    // category per round at 2 CTAs/SM beats four per round at 1 CTA/SM (4.35 vs
-    // 6.37 ms per rescore): the staging and FP64 epilogue around the UMMAs are
-    // latency-bound and need the second CTA to hide it.
-    static constexpr int RG = 1;
-    static constexpr int BYTES = RG * (2 * A_BYTES + 2 * B_BYTES) + PROD_BYTES;
-    static constexpr int COLS_USED = RG * RCOLS;
-    static constexpr int COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
-                                : COLS_USED <= 256 ? 256 : 512;
-};
-
-// one ulp of a non-negative float (0 for zero and subnormals)
-__device__ __forceinline__ double ulp_f(float f) {
-    const int e = (__float_as_int(f) >> 23) & 0xff;
-    return e == 0 ? 0.0 : pow2d(e - 127 - 23);
-}
-
-// One CTA = 128 patterns [first_tile*128 + blockIdx.x*128, +128) of op blockIdx.y.
-// A round = one child, RG categories, one 32-state half: stage, issue, wait,
-// read back.
-template <int S, int R>
-__global__ void __launch_bounds__(kTcThreads, 2) k_cla_tc(View v, LevelOps ops, int first_tile, double corr_ulps) {
-    using SM = TcSmem<S, R>;
-    constexpr int KP = SM::KP, KB = SM::KB, NH = SM::NH, RG = SM::RG;
-    constexpr int GB = 2 * SM::A_BYTES + 2 * SM::B_BYTES;  // staging bytes of one category
-    extern __shared__ __align__(1024) unsigned char tc_smem[];
-    __shared__ __align__(8) unsigned long long s_mbar;
+__global__ void __launch_bounds__(kTcThreads, 1) k_cla_i8(View v, LevelOps ops, int tile0, int ntiles) {
+    using C = I8Cfg<S, R>;
+    extern __shared__ __align__(1024) unsigned char i8_smem[];
+    __shared__ __align__(8) unsigned long long s_bar[16];
     __shared__ uint32_t s_taddr;
-    double *prod = reinterpret_cast<double *>(tc_smem + RG * GB);  // [128][RSP]
+    __shared__ int s_abort;
+    // mbarriers: 0-1 staging full (per child), 2-3 digit slot full, 4-5 slot empty,
+    // 6-8 TMEM region full, 9-11 region empty, 12-13 row exponents full, 14-15 empty
+    const uint32_t bar0 = smem_u32(&s_bar[0]);
+    auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
+    volatile int *abort = &s_abort;
     const DevOp op = ops.op[blockIdx.y];
-    const int p0 = (first_tile + blockIdx.x) * kTcM;
-    const int warp = threadIdx.x >> 5;
-    const int wg = threadIdx.x >> 7;  // warpgroup: which 8-column chunks it reads back
-    const int m = threadIdx.x & 127;  // epilogue row (TMEM lane; warp w reads lanes 32 (w % 4) ..)
-    const int p = p0 + m;
-    const uint32_t mbar = smem_u32(&s_mbar);
-    if (warp == 0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nint = op.kind == kIntInt ? 2 : op.kind == kIntTip ? 1 : 0;  // internal children: c1 (and c2)
+    const int cbuf[2] = {op.c1, op.c2};
+    const int cmat[2] = {op.p1, op.p2};
+    unsigned char *stage = i8_smem + C::OFF_STAGE;
+    unsigned char *aslot = i8_smem + C::OFF_ASLOT;
+    unsigned char *bdig = i8_smem + C::OFF_B;
+    float *outs = reinterpret_cast<float *>(i8_smem + C::OFF_OUT);
+    double *sB = reinterpret_cast<double *>(i8_smem + C::OFF_SB);
+    double *tsum = reinterpret_cast<double *>(i8_smem + C::OFF_TSUM);
+    int *eAs = reinterpret_cast<int *>(i8_smem + C::OFF_EA);
+    float *rowsc = reinterpret_cast<float *>(i8_smem + C::OFF_ROW);
+
+    if (warp == kTcEpiWarps + kTcProdWarps) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
-                     "r"((uint32_t)SM::COLS));
+                     "r"(512u));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1u));
+        s_abort = 0;
+        for (int k = 0; k < 2; k++) mbar_init(BAR(k), 1);
+        for (int k = 2; k < 6; k++) mbar_init(BAR(k), 1);
+        for (int k = 6; k < 9; k++) mbar_init(BAR(k), 1);
+        for (int k = 9; k < 12; k++) mbar_init(BAR(k), kTcEpiWarps * 32);
+        for (int k = 12; k < 14; k++) mbar_init(BAR(k), 1);
+        for (int k = 14; k < 16; k++) mbar_init(BAR(k), kTcEpiWarps * 32);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // per (child, category, row i of P_r): the row's scale 2^(eB - 22) and sum
+    // (the product of a tip with missing data), and the digits of internal children
+    for (int it = threadIdx.x; it < 2 * R * C::NPAD; it += blockDim.x) {
+        const int c = it / (R * C::NPAD), r = (it / C::NPAD) % R, i = it % C::NPAD;
+        const double *P = v.mats + (long long)cmat[c] * v.mat_stride + (long long)r * S * S;
+        double mx = 0.0, sum = 0.0;
+        if (i < S)
+            for (int j = 0; j < S; j++) {
+                const double x = __ldg(P + i * S + j);
+                mx = fmax(mx, x);
+                sum += x;
+            }
+        tsum[it] = sum;
+        const int eB = mx > 0.0 ? ilogb(mx) + 1 : 0;
+        sB[it] = pow2d(eB - 22);
+        if (c >= nint) continue;
+        unsigned char *bset = bdig + (c * R + r) * C::BSET;
+        const double sc = pow2d(38 - eB);
+        for (int j = 0; j < C::KB; j++) {
+            unsigned long long q = 0;
+            if (i < S && j < S) {
+                q = __double2ull_rn(__ldg(P + i * S + j) * sc);
+                if (q > 0x3FFFFFFFFFULL) q = 0x3FFFFFFFFFULL;
+            }
+            const unsigned long long b = (q + kDigBias) ^ kDigBias;  // balanced digits as bytes
+            const uint32_t o = i8_off(i, j, C::KB);
+#pragma unroll
+            for (int l = 0; l < kDigB; l++) bset[l * C::BPLANE + o] = (unsigned char)(b >> (8 * (4 - l)));
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = s_taddr;
-    const uint32_t trow = taddr + ((uint32_t)((warp & 3) * 32) << 16);
-    constexpr uint32_t idesc = tc_idesc(32);
-    const uint32_t sbo = KP * 32, lbo = 128;
-    bool ok = true;
-    uint32_t phase = 0;
-    for (int c = 0; c < 2 && ok; c++) {
-        const int child = c ? op.c2 : op.c1;
-        const bool tip = c ? op.kind != kIntInt : op.kind == kTipTip;
-        // a row is exact (no truncation to correct) when it is a one-hot tip state
-        bool exact_row = false;
-        if (tip && p < v.npat) exact_row = v.tips[(long long)child * v.npat_pad + p] < S;
-        for (int r0 = 0; r0 < R && ok; r0 += RG) {
-            const int ng = min(RG, R - r0);
-            for (int g = 0; g < ng; g++) {
-                unsigned char *base = tc_smem + g * GB;
-                tc_stage_a<S, R>(v, child, tip, p0, r0 + g, base, base + SM::A_BYTES);
-                tc_stage_b<S, R>(v, c ? op.p2 : op.p1, r0 + g, base + 2 * SM::A_BYTES,
-                                 base + 2 * SM::A_BYTES + SM::B_BYTES);
+    const int ntile_cta = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    auto tile_p0 = [&](int k) { return (tile0 + (int)blockIdx.x + k * (int)gridDim.x) * kTcM; };
+
+    if (warp >= kTcEpiWarps && warp < kTcEpiWarps + kTcProdWarps) {
+        // ---------------------------------------------------------------- producer
+        const int pt = threadIdx.x - kTcEpiWarps * 32;
+        const int pw = warp - kTcEpiWarps;
+        constexpr int NP = kTcProdWarps * 32;
+        constexpr bool VEC = S % 4 == 0 && C::RS % 4 == 0;  // float4 rows: 16-byte aligned groups
+        uint32_t issued = 0, waited[2] = {0, 0}, slot_cnt = 0;
+        auto issue = [&](int k) {
+            if (k >= ntile_cta) return;
+            issued++;
+            if (pt != 0) return;
+            const int p0 = tile_p0(k);
+            for (int c = 0; c < nint; c++) {
+                mbar_expect_tx(BAR(c), C::STAGE);
+                bulk_g2s(smem_u32(stage + c * C::STAGE), cla_ptr<float>(v, cbuf[c], p0, C::RS), C::STAGE, BAR(c));
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            for (int h = 0; h < NH && ok; h++) {
-                if (threadIdx.x == 0) {
-                    // B rows [32h, 32h+32) = 8-row groups 4h .. 4h+3, each SBO bytes apart
-                    const uint32_t hoff = (uint32_t)h * 4 * sbo;
-                    for (int g = 0; g < ng; g++) {
-                        const uint32_t sa = smem_u32(tc_smem + g * GB);
-                        const uint32_t ahb = sa, alb = sa + SM::A_BYTES;
-                        const uint32_t bhb = sa + 2 * SM::A_BYTES + hoff, blb = bhb + SM::B_BYTES;
-                        const uint32_t dbase = taddr + (uint32_t)(g * SM::RCOLS);
-                        for (int kb = 0; kb < KB; kb++) {
-                            const uint32_t o = kb * 256;
-                            const uint64_t ah = umma_desc(ahb + o, lbo, sbo), al = umma_desc(alb + o, lbo, sbo);
-                            const uint64_t bh = umma_desc(bhb + o, lbo, sbo), bl = umma_desc(blb + o, lbo, sbo);
-                            tc_mma(dbase + kb * 32, ah, bh, idesc, 0);       // main term, own region
-                            tc_mma(dbase + KB * 32, ah, bl, idesc, kb > 0);  // cross terms, accumulated
-                            tc_mma(dbase + KB * 32, al, bh, idesc, 1);
-                        }
-                    }
-                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-                                 : "memory");
-                }
-                ok = mbar_wait(mbar, phase & 1);
-                phase++;
-                ok = __syncthreads_and(ok) != 0;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        };
+        issue(0);
+        bool ok = true;
+        for (int k = 0; k < ntile_cta && ok; k++) {
+            const int ering = k & 1;
+            ok = group_all(tc_wait(BAR(14 + ering), ((k >> 1) & 1) ^ 1, abort), kBarProd, NP);
+            // row exponents of every (child, category) row of this tile
+            for (int c = 0; c < nint && ok; c++) {
+                ok = group_all(tc_wait(BAR(c), waited[c] & 1, abort), kBarProd, NP);
                 if (!ok) break;
-                // (P_c V_c)_s for s in [32h, 32h+32): FP64 sum of the K-step regions
-                for (int g = 0; g < ng; g++) {
-                    const uint32_t rbase = trow + (uint32_t)(g * SM::RCOLS);
-                    const int r = r0 + g;
-                    for (int c8 = wg * 8; c8 < 32; c8 += 16) {
-                        uint32_t t[KB + 1][8];
-#pragma unroll
-                        for (int kb = 0; kb <= KB; kb++) tc_ld8_nw(rbase + kb * 32 + c8, t[kb]);
-                        tc_wait_ld();
-#pragma unroll
-                        for (int j = 0; j < 8; j++) {
-                            double val = (double)__uint_as_float(t[KB][j]);
-#pragma unroll
-                            for (int kb = 0; kb < KB; kb++) {
-                                const float f = __uint_as_float(t[kb][j]);
-                                val += (double)f + (exact_row ? 0.0 : corr_ulps * ulp_f(f));
+                waited[c]++;
+                const float *row = reinterpret_cast<const float *>(stage + c * C::STAGE) + pt * C::RS;
+                for (int r = 0; r < R; r++) {
+                    uint32_t mx = 0;
+                    for (int t = 0; t < S; t++) {  // rotated start: rows at an even stride hit other banks
+                        const int j = (t + pt) % S;
+                        mx = max(mx, __float_as_uint(row[r * S + j]));
+                    }
+                    eAs[((ering * 2 + c) * R + r) * kTcM + pt] = row_exp(mx);
+                }
+            }
+            if (!ok) break;
+            ok = group_all(true, kBarProd, NP);
+            if (pt == 0) mbar_arrive(BAR(12 + ering));
+            // digit planes, one (child, category) per slot
+            for (int r = 0; r < R && ok; r++) {
+                for (int c = 0; c < nint && ok; c++) {
+                    const int s = slot_cnt & 1;
+                    ok = group_all(tc_wait(BAR(4 + s), ((slot_cnt >> 1) & 1) ^ 1, abort), kBarProd, NP);
+                    if (!ok) break;
+                    const float *tile = reinterpret_cast<const float *>(stage + c * C::STAGE);
+                    const int *eAr = eAs + ((ering * 2 + c) * R + r) * kTcM;
+                    unsigned char *dst = aslot + s * C::ASLOT;
+                    // one 8-row x 16-byte core matrix per warp and step: lane = (row, 4-byte word)
+                    for (int cm = pw; cm < (kTcM / 8) * (C::KB / 16); cm += kTcProdWarps) {
+                        const int rg = cm / (C::KB / 16), kc = cm % (C::KB / 16);
+                        const int m = rg * 8 + (lane >> 2);
+                        const int j0 = kc * 16 + (lane & 3) * 4;
+                        const int eA = eAr[m];
+                        const float *src = tile + m * C::RS + r * S + j0;
+                        unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
+                        if (VEC) {
+                            if (j0 < S) {
+                                const float4 f = *reinterpret_cast<const float4 *>(src);
+                                q[0] = fix38(__float_as_uint(f.x), eA);
+                                q[1] = fix38(__float_as_uint(f.y), eA);
+                                q[2] = fix38(__float_as_uint(f.z), eA);
+                                q[3] = fix38(__float_as_uint(f.w), eA);
                             }
-                            const int st = h * 32 + c8 + j;
-                            if (st < S) {
-                                double *q = prod + (long long)m * SM::RSP + r * S + st;
-                                *q = c ? *q * val : val;
+                        } else {
+#pragma unroll
+                            for (int t = 0; t < 4; t++)
+                                if (j0 + t < S) q[t] = fix38(__float_as_uint(src[t]), eA);
+                        }
+                        // balanced digits as bytes: digit 0 is byte 4, digits 1-4 bytes 3..0
+                        uint32_t lo[4], hi[4];
+#pragma unroll
+                        for (int t = 0; t < 4; t++) {
+                            const unsigned long long b = (q[t] + kDigBias) ^ kDigBias;
+                            lo[t] = (uint32_t)b;
+                            hi[t] = (uint32_t)(b >> 32);
+                        }
+                        const uint32_t o = i8_off(m, j0, C::KB);
+                        {
+                            const uint32_t a = __byte_perm(hi[0], hi[1], 0x40), b = __byte_perm(hi[2], hi[3], 0x40);
+                            *reinterpret_cast<uint32_t *>(dst + o) = __byte_perm(a, b, 0x5410);
+                        }
+#pragma unroll
+                        for (int d = 1; d < kDigA; d++) {
+                            // byte (4 - d) of each of the four values, packed in order
+                            const uint32_t sel = 4 - d;
+                            const uint32_t a = __byte_perm(lo[0], lo[1], sel | ((sel + 4) << 4));
+                            const uint32_t b = __byte_perm(lo[2], lo[3], sel | ((sel + 4) << 4));
+                            *reinterpret_cast<uint32_t *>(dst + d * C::APLANE + o) = __byte_perm(a, b, 0x5410);
+                        }
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    ok = group_all(true, kBarProd, NP);
+                    if (pt == 0) mbar_arrive(BAR(2 + s));
+                    slot_cnt++;
+                }
+            }
+            if (!ok) break;
+            // both staging tiles are consumed (every producer thread is past the
+            // barrier above): fetch the next tile's children
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(k + 1);
+        }
+        // copies still in flight are waited for (bounded) before the CTA can exit
+        if (pt == 0)
+            for (int c = 0; c < nint; c++)
+                for (uint32_t n = waited[c]; n < issued; n++) mbar_wait(BAR(c), n & 1);
+    } else if (warp == kTcEpiWarps + kTcProdWarps) {
+        // ---------------------------------------------------------------- MMA issuer
+        if (lane == 0 && nint > 0) {
+            uint32_t slot_cnt = 0, unit = 0;
+            bool ok = true;
+            for (int k = 0; k < ntile_cta && ok; k++) {
+                for (int r = 0; r < R && ok; r++) {
+                    int slot[2];
+                    for (int c = 0; c < nint && ok; c++) {
+                        slot[c] = slot_cnt & 1;
+                        ok = tc_wait(BAR(2 + slot[c]), (slot_cnt >> 1) & 1, abort);
+                        slot_cnt++;
+                    }
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    for (int h = 0; h < C::NH && ok; h++) {
+                        for (int c = 0; c < nint && ok; c++) {
+                            const int q = unit % kTcRegions;
+                            ok = tc_wait(BAR(9 + q), ((unit / kTcRegions) & 1) ^ 1, abort);
+                            if (!ok) break;
+                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                            const uint32_t d0 = taddr + (uint32_t)(q * kTcRegionCols);
+                            const uint32_t abase = smem_u32(aslot + slot[c] * C::ASLOT);
+                            const uint32_t bbase = smem_u32(bdig + (c * R + r) * C::BSET) + h * 4 * C::SBO;
+#pragma unroll
+                            for (int w = 0; w < kTcClasses; w++) {
+                                bool first = true;
+#pragma unroll
+                                for (int ka = 0; ka < kDigA; ka++) {
+                                    const int lb = w - ka;
+                                    if (lb < 0 || lb >= kDigB) continue;
+#pragma unroll
+                                    for (int st = 0; st < C::KSTEPS; st++) {
+                                        const uint64_t ad = umma_desc(abase + ka * C::APLANE + st * 256, 128, C::SBO);
+                                        const uint64_t bd = umma_desc(bbase + lb * C::BPLANE + st * 256, 128, C::SBO);
+                                        umma_i8(d0 + w * 32, ad, bd, first ? 0u : 1u);
+                                        first = false;
+                                    }
+                                }
                             }
+                            umma_commit(BAR(6 + q));
+                            unit++;
+                            if (h == C::NH - 1) umma_commit(BAR(4 + slot[c]));
                         }
                     }
                 }
-                // the next round's MMAs overwrite TMEM and shared memory: every read above is complete
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncthreads();
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            }
+            // every MMA issued has completed before TMEM can be freed
+            if (unit > 0) {
+                const int q = (unit - 1) % kTcRegions;
+                mbar_wait(BAR(6 + q), ((unit - 1) / kTcRegions) & 1);
             }
         }
-    }
-    if (!ok) {
-        if (threadIdx.x == 0) atomicOr(v.status, kStatusTcTimeout);
+        __syncwarp();
     } else {
-        // row m: each warpgroup takes half of the R*S entries; the row max is combined in shared
-        // memory (the staging area, free once the last products are read back)
-        double(*s_mx)[kTcM] = reinterpret_cast<double(*)[kTcM]>(tc_smem);
-        const double *row = prod + (long long)m * SM::RSP;
-        const int k0 = wg ? (R * S) / 2 : 0, k1 = wg ? R * S : (R * S) / 2;
-        double mx = 0.0;
-        for (int k = k0; k < k1; k++) mx = fmax(mx, row[k]);
-        s_mx[wg][m] = mx;
-        __syncthreads();
-        mx = fmax(s_mx[0][m], s_mx[1][m]);
-        if (p < v.npat) {
+        // ---------------------------------------------------------------- epilogue
+        const int m = threadIdx.x;  // TMEM lane = pattern row of the tile
+        const uint32_t trow = taddr + ((uint32_t)(warp * 32) << 16);
+        uint32_t unit = 0;
+        for (int k = 0; k < ntile_cta; k++) {
+            const int p0 = tile_p0(k), p = p0 + m;
+            const bool live = p < v.npat;
+            const int ering = k & 1;
+            if (!group_all(tc_wait(BAR(12 + ering), (k >> 1) & 1, abort), kBarEpi, kTcEpiWarps * 32)) break;
+            int code[2] = {S, S};
+            for (int c = nint; c < 2; c++)
+                if (live) code[c] = v.tips[(long long)cbuf[c] * v.npat_pad + p];
+            float *dst_tile = cla_ptr<float>(v, op.dest, p0, C::RS);
+            double mx = 0.0;
+            bool ok = true;
+            for (int r = 0; r < R && ok; r++) {
+                double ea[2] = {1.0, 1.0};
+                for (int c = 0; c < nint; c++) ea[c] = pow2d(eAs[((ering * 2 + c) * R + r) * kTcM + m] - 22);
+                for (int h = 0; h < C::NH && ok; h++) {
+                    int q[2] = {0, 0};
+                    for (int c = 0; c < nint; c++) {
+                        q[c] = unit % kTcRegions;
+                        ok = ok && tc_wait(BAR(6 + q[c]), (unit / kTcRegions) & 1, abort);
+                        unit++;
+                    }
+                    // the warp's TMEM reads below are warp-collective: its lanes decide together
+                    ok = __all_sync(0xffffffffu, ok);
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                        if (h * 32 + c8 >= S) break;  // uniform across the warp
+                        double d[2][8];
+                        for (int c = 0; c < 2; c++) {
+                            if (c < nint) {
+                                uint32_t t[kTcClasses][8];
+#pragma unroll
+                                for (int w = 0; w < kTcClasses; w++)
+                                    tmem_ld8(trow + (uint32_t)(q[c] * kTcRegionCols + w * 32 + c8), t[w]);
+                                tmem_wait_ld();
+#pragma unroll
+                                for (int j = 0; j < 8; j++) {
+                                    const long long acc = (long long)(int)t[0][j] * (1ll << 32) +
+                                                          (long long)(int)t[1][j] * (1ll << 24) +
+                                                          (long long)(int)t[2][j] * (1ll << 16) +
+                                                          (long long)(int)t[3][j] * (1ll << 8) + (long long)(int)t[4][j];
+                                    const int i = min(h * 32 + c8 + j, C::NPAD - 1);
+                                    // the exact product is >= 0; the dropped classes may leave a tiny negative
+                                    d[c][j] = fmax(0.0, (double)acc * sB[(c * R + r) * C::NPAD + i] * ea[c]);
+                                }
+                            } else {
+                                const double *P = v.mats + (long long)cmat[c] * v.mat_stride + (long long)r * S * S;
+#pragma unroll
+                                for (int j = 0; j < 8; j++) {
+                                    const int i = h * 32 + c8 + j;
+                                    double x = 0.0;
+                                    if (i < S)
+                                        x = code[c] < S ? __ldg(P + i * S + code[c]) : tsum[(c * R + r) * C::NPAD + i];
+                                    d[c][j] = x;
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; j++) {
+                            const int i = h * 32 + c8 + j;
+                            if (i < S) {
+                                const double x = d[0][j] * d[1][j];
+                                mx = fmax(mx, x);
+                                const int idx = r * S + i;
+                                const unsigned int key =
+                                    (unsigned int)(reinterpret_cast<unsigned long long>(dst_tile + m * C::RS + idx) >> 2);
+                                outs[m * C::RSP + idx] = live ? round_stochastic_exact(x, key) : 0.f;
+                            }
+                        }
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    for (int c = 0; c < nint; c++) mbar_arrive(BAR(9 + q[c]));
+                }
+            }
+            mbar_arrive(BAR(14 + ering));
+            ok = group_all(ok, kBarEpi, kTcEpiWarps * 32);
+            if (!ok) break;
+            // power-of-two normalisation of each pattern and its scaler
             int e = 0;
-            if (mx > 0.0) e = max(-1000, min(1000, ilogb(mx)));
-            const double sc = pow2d(-e);
-            float *dst = cla_ptr<float>(v, op.dest, p, R * S);
-            for (int k = k0; k < k1; k++)
-                dst[k] = round_stochastic_exact(row[k] * sc,
-                                                (unsigned int)(reinterpret_cast<unsigned long long>(dst + k) >> 2));
-            if (wg == 0) {
+            if (mx > 0.0) e = max(-126, min(126, ilogb(mx)));
+            if (live && mx > 0.0 && mx < 5.421010862427522e-20) atomicOr(v.status, kStatusTcRange);  // 2^-64
+            rowsc[m] = __int_as_float((127 - e) << 23);
+            if (live) {
                 int ms = 0;
                 if (op.kind != kTipTip) ms += v.scalers[(long long)op.c1 * v.npat_pad + p];
                 if (op.kind == kIntInt) ms += v.scalers[(long long)op.c2 * v.npat_pad + p];
                 v.scalers[(long long)op.dest * v.npat_pad + p] = ms - e;
             }
+            group_all(true, kBarEpi, kTcEpiWarps * 32);
+            // coalesced store of the tile (rows beyond the last pattern are skipped)
+            const int nrow = min(kTcM, v.npat - p0);
+            for (int x = m; x < nrow * C::RS; x += kTcEpiWarps * 32) {
+                const int row = x / C::RS, col = x - row * C::RS;
+                dst_tile[x] = outs[row * C::RSP + col] * rowsc[row];
+            }
+            group_all(true, kBarEpi, kTcEpiWarps * 32);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"((uint32_t)SM::COLS));
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0 && s_abort) atomicOr(v.status, kStatusTcTimeout);
+    if (warp == kTcEpiWarps + kTcProdWarps)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(512u));
 }
 
 }  // namespace gb

@@ -110,7 +110,6 @@ SIGNATURES = {
     "gb_get_batch_tuning": (C.c_int, [C.c_int, _I]),
     "gb_get_batch_timing": (C.c_int, [C.c_int, _D]),
     "gb_set_tensor_cores": (C.c_int, [C.c_int, C.c_int]),
-    "gb_set_tensor_core_correction": (C.c_int, [C.c_int, C.c_double]),
     "gb_set_buffer_precision": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "gb_set_eigen_from_rate_matrices": (C.c_int, [C.c_int, C.c_int, _I, _D, _D, _D, _I]),
     "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),

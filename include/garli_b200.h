@@ -213,14 +213,15 @@ int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 /* Newton state of one matrix after a pass: length, improvement, lnL, d1, d2, evaluations */
 int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
-/* precision form, 20 and 61 states: 1 (default) = CLA updates of the FP32
- * segment on the tensor cores (tcgen05.mma kind::tf32, 3xTF32 split products,
- * FP32 accumulation in TMEM); 0 = the CUDA-core FP64-arithmetic kernel */
+/* precision form, 20 states (up to 4 categories) and 61 states (one
+ * category): 1 (default) = CLA updates of the FP32 segment on the tensor cores
+ * (tcgen05.mma kind::i8: the CLA as 4 and P(t) as 5 base-256 digits over
+ * per-row power-of-two scales, exact 32-bit integer accumulation, each P.CLA
+ * product within 2.5e-10 of the CLA row's largest entry); 0 = the CUDA-core
+ * FP64-arithmetic kernel.  A pattern whose product maximum falls below 2^-64
+ * switches the instance to the CUDA-core kernel (the score that saw it returns
+ * GB_ERROR_RESCALE_RETRY, and the tree drivers redo it). */
 int gb_set_tensor_cores(int instance, int on);
-/* calibration of the tensor-core path: the mean loss, in ulps of the result,
- * that one tensor-core FP32 result carries from its truncating accumulation;
- * it is added back to every inexact K-step result (0 .. 8) */
-int gb_set_tensor_core_correction(int instance, double ulps);
 
 /* ---- batched candidate scoring and branch optimisation (4 states) ----
  * A GA generation's candidates (population.cpp:4532-4589: each mutated

@@ -92,7 +92,6 @@ def test_new_entry_points_reject_bad_handles_and_sizes_without_device():
     assert L.gb_set_batch_tuning(4321, 1, 1) == -4
     assert L.gb_get_batch_tuning(4321, i4) == -4
     assert L.gb_set_tensor_cores(4321, 1) == -4
-    assert L.gb_set_tensor_core_correction(4321, 0.5) == -4
     assert L.gb_set_buffer_precision(4321, 10, 1) == -4
     assert L.gb_set_eigen_from_rate_matrices(4321, 1, i4, d3, d3, d3, None) == -4
     assert L.gbp_score_candidates(4321, 1, i4, d3, i4, 0.01, 0, d3, d3) == -4
