@@ -118,6 +118,7 @@ struct Instance {
     unsigned long long bgraph_key = 0;
     int use_batch_graph = 1;
     int use_tc = 1;  // precision form, 20 / 61 states: CLA updates on the tensor cores
+    unsigned char *d_tctab = nullptr;  // per-op P digit tables of a tensor-core level (k_pdigits)
     double batch_ms = 0.0;  // CUDA-event time of the timed batched launches
     long long batch_timed = 0;
     // per-phase timing of the batched pass (levels, coefficient passes, Newton /
@@ -233,6 +234,13 @@ static int ns_cla_tile(const Instance *I, size_t *smem) {
     *smem = (size_t)(2 * RSS + 3 * tp * RS + tp) * 8;
     return tp;
 }
+// the precision form's FP64 pattern segment beside the tensor-core kernel: a
+// few hundred patterns, so small tiles (many blocks) rather than deep ones
+static int ns_seg_tile(const Instance *I, size_t *smem) {
+    const int RS = I->R * I->S, RSS = RS * I->S, tp = 8;
+    *smem = (size_t)(2 * RSS + 3 * tp * RS + tp) * 8;
+    return tp;
+}
 static int ns_edge_tile(const Instance *I, size_t *smem) {
     const int RS = I->R * I->S, RSS = RS * I->S;
     int tp = 64;
@@ -247,17 +255,23 @@ static int ns_edge_tile(const Instance *I, size_t *smem) {
 static bool tc_supported(const Instance *I) {
     return I->mixed && I->use_tc && ((I->S == 20 && I->R <= 4) || (I->S == 61 && I->R == 1));
 }
-static void *tc_func(int S, int R, size_t *smem) {
-#define GB_TC(s, r)                                  \
-    if (S == s && R == r) {                          \
-        *smem = I8Cfg<s, r>::BYTES;                  \
-        return (void *)k_cla_i8<s, r>;               \
+// the CLA kernel (dynamic shared memory in *smem) and its per-level table
+// kernel k_pdigits (*prep)
+static void *tc_func(int S, int R, size_t *smem, void **prep = nullptr) {
+#define GB_TC(s, r)                                      \
+    if (S == s && R == r) {                              \
+        *smem = I8Cfg<s, r>::BYTES;                      \
+        if (prep) *prep = (void *)k_pdigits<s, r>;       \
+        return (void *)k_cla_i8<s, r>;                   \
     }
     GB_TC(20, 1) GB_TC(20, 2) GB_TC(20, 3) GB_TC(20, 4) GB_TC(61, 1)
 #undef GB_TC
     *smem = 0;
     return nullptr;
 }
+// bytes of the per-op tables of a level (k_pdigits output), for any supported shape
+constexpr size_t kTcTableBytes = (size_t)kMaxLevelOps * 48 * 1024;
+static_assert(I8Cfg<20, 4>::OPB <= 48 * 1024 && I8Cfg<61, 1>::OPB <= 48 * 1024, "tensor-core table slot");
 // grid of a tensor-core level launch: tiles per op split so that the level
 // fills the SMs about twice over (one CTA per SM at a time; each CTA runs a
 // pipeline over its tiles of one op)
@@ -339,9 +353,9 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             GB_CUDA(cudaLaunchKernel(cla4_func(I->R, !I->mixed), grid, dim3(kThreads), args, 0, I->stream));
         } else {
             size_t smem;
-            const int tp = ns_cla_tile(I, &smem);
             // precision form on the tensor cores: CUDA cores keep only the FP64 segment
             const bool tc = tc_supported(I);
+            const int tp = tc ? ns_seg_tile(I, &smem) : ns_cla_tile(I, &smem);
             const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
             if (ns_pat > 0) {
                 dim3 grid((ns_pat + tp - 1) / tp, L.n);
@@ -351,8 +365,12 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             int first = I->kpad / kTcM, nt = I->npat_pad / kTcM - first;
             if (tc && nt > 0) {
                 size_t tsm = 0;
-                void *f = tc_func(I->S, I->R, &tsm);
-                void *args[] = {&v, &L, (void *)&first, (void *)&nt};
+                void *prep = nullptr;
+                void *f = tc_func(I->S, I->R, &tsm, &prep);
+                const unsigned char *tab = I->d_tctab;
+                void *pargs[] = {&v, &L, (void *)&tab};
+                GB_CUDA(cudaLaunchKernel(prep, dim3(L.n), dim3(kThreads), pargs, 0, I->stream));
+                void *args[] = {&v, &L, (void *)&first, (void *)&nt, (void *)&tab};
                 GB_CUDA(cudaLaunchKernel(f, tc_grid(I, nt, L.n), dim3(kTcThreads), args, tsm, I->stream));
             }
         }
@@ -507,6 +525,7 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         {(void **)&I->d_slots, (size_t)I->nmat * sizeof(NrSlot)},
         {(void **)&I->d_gsync, sizeof(GridSync)},
         {(void **)&I->d_sums2, (size_t)2 * 3 * kMaxScoreBlocks * sizeof(double)},
+        {(void **)&I->d_tctab, (I->mixed && I->S != 4) ? kTcTableBytes : (size_t)16},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, a.n) != cudaSuccess) {
@@ -570,7 +589,8 @@ int gb_finalize_instance(int instance) {
                     I->d_eigen, I->d_freqs, I->d_rates, I->d_rprobs, I->d_status, I->d_block_sums,
                     I->d_result, I->d_site_lnl, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
                     I->d_cmds, I->d_pops, I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots,
-                    I->d_chunk_sums, I->d_active, I->d_mentries, I->d_coef, I->d_etab, I->d_cscale};
+                    I->d_chunk_sums, I->d_active, I->d_mentries, I->d_coef, I->d_etab, I->d_cscale,
+                    I->d_tctab};
     if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
     if (I->bgraph) cudaGraphDestroy(I->bgraph);
     for (void *p : ptrs)
@@ -1212,21 +1232,27 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                     rc = B.add(B.g, &prev, cla4_func(I->R, garli), cla4_grid(I, L.n), 0, args);
                 } else {
                     int S = I->S, R = I->R, tp = ns_tp;
+                    size_t smem = ns_smem;
                     const bool tc = tc_supported(I);
+                    if (tc) tp = ns_seg_tile(I, &smem);
                     const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
                     if (ns_pat > 0) {
                         void *args[] = {&v, &L, &S, &R, &tp};
                         rc = B.add(B.g, &prev, garli ? (void *)k_cla_ns<true> : (void *)k_cla_ns<false>,
-                                   dim3((ns_pat + ns_tp - 1) / ns_tp, L.n), ns_smem, args);
+                                   dim3((ns_pat + tp - 1) / tp, L.n), smem, args);
                     }
                     int first = I->kpad / kTcM;
                     int nt = I->npat_pad / kTcM - first;
                     if (!rc && tc && nt > 0) {
                         size_t tsm = 0;
-                        void *f = tc_func(I->S, I->R, &tsm);
-                        void *args[] = {&v, &L, &first, &nt};
+                        void *prep = nullptr;
+                        void *f = tc_func(I->S, I->R, &tsm, &prep);
+                        unsigned char *tab = I->d_tctab;
+                        void *pargs[] = {&v, &L, &tab};
+                        rc = B.add(B.g, &prev, prep, dim3(L.n), 0, pargs);
+                        void *args[] = {&v, &L, &first, &nt, &tab};
                         B.block = dim3(kTcThreads);
-                        rc = B.add(B.g, &prev, f, tc_grid(I, nt, L.n), tsm, args);
+                        if (!rc) rc = B.add(B.g, &prev, f, tc_grid(I, nt, L.n), tsm, args);
                         B.block = dim3(kThreads);
                     }
                 }
