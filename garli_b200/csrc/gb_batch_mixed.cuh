@@ -580,12 +580,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_cla4m(View v, LevelOps ops) {
 // op, blockIdx.x = a run of tpi tiles, inputs prefetched as in the persistent
 // kernel's levels.
 template <int R>
-__global__ void __launch_bounds__(kThreads, 4) k_level4m(View v, const DevOp *ops, int tpi) {
+__device__ __forceinline__ void level4m_body(const View &v, const DevOp &op, int tpi) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     __shared__ double sP[2][R][kPStride];
     extern __shared__ __align__(128) unsigned char dsm[];  // cp_smem_bytes() of prefetch slots
-    const DevOp op = ops[blockIdx.y];
     for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
         const int mi = q / (R * 16), rem = q % (R * 16);
         sP[mi][rem / 16][rem % 16] = __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
@@ -597,6 +596,16 @@ __global__ void __launch_bounds__(kThreads, 4) k_level4m(View v, const DevOp *op
     const int ctiles = (v.npat + PPB - 1) / PPB;
     const int t0 = blockIdx.x * tpi;
     cla_tiles_cp<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ctiles, t0 + tpi), crr, ok, dsm);
+}
+template <int R>
+__global__ void __launch_bounds__(kThreads, 4) k_level4m(View v, const DevOp *ops, int tpi) {
+    level4m_body<R>(v, ops[blockIdx.y], tpi);
+}
+// the same level launch with the ops passed by value (the per-tree precision
+// form: its levels come from gb_update_partials, not a device queue)
+template <int R>
+__global__ void __launch_bounds__(kThreads, 4) k_level4m_ops(View v, LevelOps ops, int tpi) {
+    level4m_body<R>(v, ops.op[blockIdx.y], tpi);
 }
 
 // A coefficient pass as a launch of its own, between the persistent kernel's

@@ -280,6 +280,7 @@ static dim3 tc_grid(const Instance *I, int ntiles, int nops) {
     return dim3(std::max(1, std::min(ntiles, want)), nops);
 }
 
+static void *level4m_ops_func(int R);
 static int set_smem_attrs() {
     const int big = 200 * 1024;
     GB_CUDA(cudaFuncSetAttribute(k_eigen_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -297,6 +298,10 @@ static int set_smem_attrs() {
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_pmats, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    for (int R = 1; R <= 8; R++)
+        GB_CUDA(cudaFuncSetAttribute(level4m_ops_func(R), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     cp_smem_bytes()));
+    GB_CUDA(cudaFuncSetAttribute(k_pmat_len, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     return GB_SUCCESS;
 }
 
@@ -334,6 +339,26 @@ static dim3 cla4_grid(const Instance *I, int nops) {
 
 static void *cla4_func(int R, bool garli);
 
+// the precision form's per-tree CLA level (k_level4m_ops: the batched pass's
+// prefetched level code): grid (runs of tpi tiles, ops), about four waves of
+// four CTAs per SM
+static void *level4m_ops_func(int R) {
+#define GB_CASE(r) \
+    case r: return (void *)k_level4m_ops<r>;
+    switch (R) {
+        GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
+    }
+#undef GB_CASE
+}
+static dim3 level4m_grid(const Instance *I, int nops, int *tpi) {
+    const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
+    const int ctiles = (I->npat + kThreads / G - 1) / (kThreads / G);
+    const long long want = 16LL * I->nsm;  // blocks in the launch
+    const long long t = ((long long)ctiles * nops + want - 1) / want;
+    *tpi = (int)std::max(1LL, std::min(32LL, t));
+    return dim3((ctiles + *tpi - 1) / *tpi, nops);
+}
+
 static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleEvery) {
     View v = make_view(I);
     v.rescale_every = rescaleEvery;
@@ -347,7 +372,13 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             cudaEventCreate(&e1);
             cudaEventRecord(e0, I->stream);
         }
-        if (I->S == 4) {
+        if (I->S == 4 && I->mixed) {
+            int tpi = 1;
+            const dim3 grid = level4m_grid(I, L.n, &tpi);
+            void *args[] = {&v, &L, &tpi};
+            GB_CUDA(cudaLaunchKernel(level4m_ops_func(I->R), grid, dim3(kThreads), args, cp_smem_bytes(),
+                                     I->stream));
+        } else if (I->S == 4) {
             const dim3 grid = cla4_grid(I, L.n);
             void *args[] = {&v, &L};
             GB_CUDA(cudaLaunchKernel(cla4_func(I->R, !I->mixed), grid, dim3(kThreads), args, 0, I->stream));
@@ -777,9 +808,10 @@ int gb_update_transition_matrices(int instance, const gb_transmat_operation *ops
             T.op[i].derivs = o.calcDerivs;
             T.op[i].t = o.edgeLength;
         }
-        const size_t smem = 3 * (size_t)I->R * I->S * sizeof(double);
-        k_pmats<<<T.n, kThreads, smem, I->stream>>>(I->d_eigen, I->eig_stride(), I->S, I->R, I->d_rates, I->pinv,
-                                                     I->has_pinv, T, I->d_mats, I->mat_stride());
+        const size_t smem = pmat_smem_bytes(I->S, I->R);
+        k_pmats<<<dim3(T.n, pmat_chunks(I->S, I->R)), kThreads, smem, I->stream>>>(
+            I->d_eigen, I->eig_stride(), I->S, I->R, I->d_rates, I->pinv, I->has_pinv, T, I->d_mats,
+            I->mat_stride());
         int rc = check_launch(I);
         if (rc) return rc;
     }
@@ -1212,7 +1244,7 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
         ns_edge_tp = ns_edge_tile(I, &ns_edge_smem);
     }
     const int nblocks = dna ? I->nvb4 : std::min(kMaxScoreBlocks, (I->npat + ns_edge_tp - 1) / ns_edge_tp);
-    const size_t pmat_smem = 3 * (size_t)I->R * I->S * sizeof(double);
+    const size_t pmat_smem = pmat_smem_bytes(I->S, I->R);
     int rc;
     {
         int n = I->nmat;
@@ -1227,7 +1259,12 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                 LevelOps L;
                 L.n = (int)std::min<size_t>(kMaxLevelOps, lv.size() - c);
                 for (int i = 0; i < L.n; i++) L.op[i] = lv[c + i];
-                if (dna) {
+                if (dna && !garli) {
+                    int tpi = 1;
+                    const dim3 grid = level4m_grid(I, L.n, &tpi);
+                    void *args[] = {&v, &L, &tpi};
+                    rc = B.add(B.g, &prev, level4m_ops_func(I->R), grid, cp_smem_bytes(), args);
+                } else if (dna) {
                     void *args[] = {&v, &L};
                     rc = B.add(B.g, &prev, cla4_func(I->R, garli), cla4_grid(I, L.n), 0, args);
                 } else {
@@ -1303,7 +1340,7 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                 int S = I->S, R = I->R, hp = I->has_pinv, e0 = 0;
                 double pinv = I->pinv;
                 void *args[] = {&I->d_eigen, &es, &S, &R, &I->d_rates, &pinv, &hp, &mat, &e0, &I->d_len, &I->d_mats, &ms};
-                rc = B.add(body, &bprev, (void *)k_pmat_len, dim3(1), pmat_smem, args);
+                rc = B.add(body, &bprev, (void *)k_pmat_len, dim3(pmat_chunks(I->S, I->R)), pmat_smem, args);
                 if (rc) return rc;
             }
         }

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kThreads) k_nr_iter4(View v, NrSlot *slot, int
     op.eigen = 0;
     op.derivs = 1;
     op.t = s_len;
-    pmat_body(eig, eig_stride, 4, R, rates, v.pinv, v.has_pinv, op, const_cast<double *>(v.mats), v.mat_stride);
+    pmat_body(eig, eig_stride, 4, R, rates, v.pinv, v.has_pinv, op, const_cast<double *>(v.mats), v.mat_stride, 0, 1);
 }
 
 }  // namespace gb

@@ -24,9 +24,19 @@ struct TransOps {
 // P_ij = max(0, sum_k (U_ik Uinv_kj) e_k) with the k sum sequential.
 // eig layout per eigen index: [lambda (S) | U (S*S) | Uinv (S*S)], lambda pre-scaled
 // by the blen multiplier.
+// outputs per block of one matrix: R*S*S split over pmat_chunks(S, R) blocks
+__host__ __device__ constexpr int pmat_chunks(int S, int R) {
+    return (R * S * S + 511) / 512 < 16 ? (R * S * S + 511) / 512 : 16;
+}
+// dynamic shared memory of a P(t) block: the exponential tables and, for 20
+// and 61 states, U and U^-1 (read S times per output)
+__host__ __device__ constexpr size_t pmat_smem_bytes(int S, int R) {
+    return (3 * (size_t)R * S + (S > 4 ? 2 * (size_t)S * S : 0)) * sizeof(double);
+}
+
 __device__ __forceinline__ void pmat_body(const double *eig, long long eig_stride, int S, int R,
                                           const double *rates, double pinv, int has_pinv, const TransOp op,
-                                          double *mats, long long mat_stride) {
+                                          double *mats, long long mat_stride, int chunk, int nchunks) {
     extern __shared__ double sh[];
     double *ex = sh, *d1e = ex + R * S, *d2e = d1e + R * S;
     const double *lam = eig + (long long)op.eigen * eig_stride;
@@ -40,10 +50,20 @@ __device__ __forceinline__ void pmat_body(const double *eig, long long eig_strid
         d1e[idx] = mul(sev, e);
         d2e[idx] = mul(sev, d1e[idx]);
     }
+    if (S > 4) {
+        double *sU = d2e + R * S, *sUi = sU + S * S;
+        for (int idx = threadIdx.x; idx < S * S; idx += blockDim.x) {
+            sU[idx] = U[idx];
+            sUi[idx] = Ui[idx];
+        }
+        U = sU;
+        Ui = sUi;
+    }
     __syncthreads();
     double *out = mats + (long long)op.dest * mat_stride;
-    const int SS = S * S;
-    for (int idx = threadIdx.x; idx < R * SS; idx += blockDim.x) {
+    const int SS = S * S, n = R * SS, per = (n + nchunks - 1) / nchunks;
+    const int i0 = chunk * per, i1 = min(n, i0 + per);
+    for (int idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
         const int r = idx / SS, ij = idx % SS, i = ij / S, j = ij % S;
         const double *e = ex + r * S;
         double sp = 0.0, s1 = 0.0, s2 = 0.0;
@@ -63,14 +83,16 @@ __device__ __forceinline__ void pmat_body(const double *eig, long long eig_strid
     }
 }
 
+// grid (matrices, pmat_chunks(S, R))
 __global__ void __launch_bounds__(kThreads) k_pmats(const double *eig, long long eig_stride, int S, int R,
                                                     const double *rates, double pinv, int has_pinv,
                                                     TransOps ops, double *mats, long long mat_stride) {
-    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, ops.op[blockIdx.x], mats, mat_stride);
+    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, ops.op[blockIdx.x], mats, mat_stride, blockIdx.y,
+              gridDim.y);
 }
 
 // P(t), dP/dt, d2P/dt2 of one matrix whose branch length lives on the device
-// (the Newton iterations of a device-side optimisation pass)
+// (the Newton iterations of a device-side optimisation pass); grid pmat_chunks(S, R)
 __global__ void __launch_bounds__(kThreads) k_pmat_len(const double *eig, long long eig_stride, int S, int R,
                                                        const double *rates, double pinv, int has_pinv, int dest,
                                                        int eigen, const double *lengths, double *mats,
@@ -80,7 +102,7 @@ __global__ void __launch_bounds__(kThreads) k_pmat_len(const double *eig, long l
     op.eigen = eigen;
     op.derivs = 1;
     op.t = lengths[dest];
-    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, op, mats, mat_stride);
+    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, op, mats, mat_stride, blockIdx.x, gridDim.x);
 }
 
 // Sum the per-block partial sums of an edge evaluation (nblocks x 3) into

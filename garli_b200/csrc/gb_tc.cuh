@@ -184,24 +184,23 @@ __device__ __forceinline__ bool group_all(bool ok, int id, int n) {
     return r != 0;
 }
 
-// bounded wait that also gives up as soon as another role has given up
+// bounded wait that also gives up as soon as another role has given up.  Each
+// try_wait suspends the thread until the phase completes or 20 microseconds
+// pass (a waiting warp takes no issue slots from the warps doing the work);
+// after about two seconds the wait gives up and raises the abort flag.
 __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile int *abort) {
-    unsigned long long t0 = 0;
-    for (long long it = 0; it < (1LL << 24); it++) {
+    const unsigned long long t0 = stage_ns();
+    for (int it = 0; it < (1 << 20); it++) {
         uint32_t done;
         asm volatile(
-            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
             "selp.b32 %0, 1, 0, P1;\n\t}\n"
             : "=r"(done)
-            : "r"(mbar), "r"(parity)
+            : "r"(mbar), "r"(parity), "r"(20000u)
             : "memory");
         if (done) return true;
-        if ((it & 255) == 0) {
-            if (*abort) return false;
-            const unsigned long long t = stage_ns();
-            if (it == 0) t0 = t;
-            else if (t - t0 > 2000000000ULL) break;
-        }
+        if (*abort) return false;
+        if (stage_ns() - t0 > 2000000000ULL) break;
     }
     *abort = 1;
     return false;
