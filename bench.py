@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--precision", type=float, default=0.01, help="Newton optPrecision")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single", action="store_true", help="skip the single-tree secondary measurement")
+    ap.add_argument("--tuning", default="",
+                    help="profiling: fixed work-item sizes 'tiles,chunks' of the batched pass (no autotuning)")
     ap.add_argument("--batch-only", action="store_true",
                     help="profiling: only the batched form (no per-tree comparison, no e2e pass)")
     ap.add_argument("--nstate-only", action="store_true",
@@ -255,6 +257,8 @@ def run_batch(bw, args, device, mixed, sequential, steps, warmup, clocks=None):
 
     w, c3s, dls, conn = bw
     inst, pop = engine.population_engine(w.data, w.child3, w.dlen, w.model, len(conn), device=device, mixed=mixed)
+    if args.tuning:
+        pop.set_tuning(*[int(x) for x in args.tuning.split(",")])
     stream = torch.cuda.ExternalStream(inst.stream_ptr(), device=f"cuda:{device}")
     out = lens = None
     for _ in range(warmup):  # the first call computes the base tree's CLAs and autotunes
@@ -417,10 +421,20 @@ def nstate_forms(kind, device, reps=3):
         torch.cuda.synchronize(device)
         ms = e0.elapsed_time(e1)
         upd = tree.counters()["pattern_updates"] - c0["pattern_updates"]
+        # CLA kernels alone: algorithmic bytes (by op kind) over their CUDA-event time
+        inst.set_kernel_timing(True)
+        for _ in range(2):
+            tree.make_all_dirty()
+            tree.score(0)
+        inst.synchronize()
+        kt = inst.kernel_timing()
+        inst.set_kernel_timing(False)
+        gbs = kt["cla_bytes"] / (kt["cla_ms"] / 1000.0) / 1e9 if kt["cla_ms"] > 0 else None
         if ref is None:
             ref = lnl
         out[name] = {"site_updates_per_s": upd / (ms / 1000.0), "ms_per_rescore": ms / reps, "lnl": lnl,
-                     "dlnl_vs_plain": lnl - ref}
+                     "dlnl_vs_plain": lnl - ref, "cla_kernel_gbs": gbs,
+                     "cla_hbm_frac": gbs / peaks()[0] if gbs else None}
         tree.close()
         inst.close()
     return out
@@ -642,7 +656,8 @@ def main():
         if rank == 0:
             print(json.dumps({"batch_only": True, "value": r["updates"] / (r["ms"] / 1000.0), "unit": UNIT,
                               "ms_per_step": r["ms"] / args.steps, "npat": w.data.npat,
-                              "alg_bytes_per_launch": r["counters"]["alg_bytes"], "tuning": r["tuning"]}))
+                              "alg_bytes_per_pass": r["counters"]["alg_bytes"], "tuning": r["tuning"],
+                              "launches_per_step": r["launches"] / max(1, args.steps)}))
         r["pop"].close()
         r["inst"].close()
         if pg:

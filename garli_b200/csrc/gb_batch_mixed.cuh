@@ -143,7 +143,8 @@ __device__ __forceinline__ void cla_finish_m(const View &v, int dest, bool wide,
         st4d(cla_ptr<double>(v, dest, p, R * 4) + r * 4, d);
     } else {
         float *q = cla_ptr<float>(v, dest, p, R * 4) + r * 4;
-        const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(q) >> 4);
+        // keyed on the slice's offset in the CLA pool: the same rounding in every run
+        const unsigned int key = (unsigned int)((reinterpret_cast<const char *>(q) - v.partials) >> 4);
         reinterpret_cast<float4 *>(q)[0] = round_stochastic4(d, key);
     }
     if (r == 0) v.scalers[(long long)dest * v.npat_pad + p] = m - e;

@@ -988,6 +988,12 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
         GB_CUDA(cudaStreamSynchronize(I->stream));
         return GB_ERROR_RESCALE_RETRY;
     }
+    if (*I->h_status & kStatusBarrierTimeout) {
+        GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        g_last_error = "CLA level: a prefetch wait exceeded its bound";
+        return GB_ERROR_GENERAL;
+    }
     if (*I->h_status & kStatusTcTimeout) {
         GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
         GB_CUDA(cudaStreamSynchronize(I->stream));

@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S
         float *dst = cla_ptr<float>(v, op.dest, p0, RS);
         for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
             const double mult = mx[o / RS];
-            const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(dst + o) >> 2);
+            // keyed on the value's offset in the CLA pool: the same rounding in every run
+            const unsigned int key = (unsigned int)((reinterpret_cast<const char *>(dst + o) - v.partials) >> 2);
             dst[o] = round_stochastic(mult != 1.0 ? mul(D[o], mult) : D[o], key);
         }
     }
