@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgarli_b200.so")
 
-SOURCES = ["gb_engine.cu", "gb_model.cpp", "gb_tree.cpp", "gb_population.cpp", "gb_noalloc.cu"]
+SOURCES = ["gb_engine.cu", "gb_model.cpp", "gb_tree.cpp", "gb_modelopt.cpp", "gb_population.cpp", "gb_noalloc.cu"]
 HEADERS = ["gb_common.cuh", "gb_dna.cuh", "gb_nstate.cuh", "gb_pmat.cuh", "gb_newton.h", "gb_graph.cuh",
            "gb_newton_dna.cuh", "gb_persist.cuh", "gb_batch.cuh", "gb_batch_mixed.cuh", "gb_tc.cuh", "gb_persist_mixed.cuh", "gb_eigen.cuh", "gb_stage.cuh"]
 GENCODE = "-gencode=arch=compute_100a,code=sm_100a"

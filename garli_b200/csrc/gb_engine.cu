@@ -119,6 +119,17 @@ struct Instance {
     int use_batch_graph = 1;
     int use_tc = 1;  // precision form, 20 / 61 states: CLA updates on the tensor cores
     unsigned char *d_tctab = nullptr;  // per-op P digit tables of a tensor-core level (k_pdigits)
+    // model slots, one per eigen index (model_slot_stride doubles each): the
+    // instance-wide setters write every slot, gb_set_model_slot one
+    std::vector<double> h_mslots;
+    double *d_mslots = nullptr;
+    double *d_multi = nullptr;  // results of gb_calculate_edges, 3 per edge
+    size_t cap_multi = 0;
+    // scratch of gb_set_eigen_from_rate_matrices, kept between calls
+    double *d_eq = nullptr, *d_epi = nullptr;
+    EigenJob *d_ejobs = nullptr;
+    int *d_esw = nullptr;
+    int cap_eig = 0;
     double batch_ms = 0.0;  // CUDA-event time of the timed batched launches
     long long batch_timed = 0;
     // per-phase timing of the batched pass (levels, coefficient passes, Newton /
@@ -163,7 +174,9 @@ static int check_launch(Instance *I) {
     return GB_SUCCESS;
 }
 
-static View make_view(Instance *I) {
+// model slot `slot` supplies the state frequencies, category weights and the
+// invariant-sites term (slot 0 = the instance-wide model)
+static View make_view(Instance *I, int slot = 0) {
     View v;
     v.partials = reinterpret_cast<char *>(I->d_partials);
     v.scalers = I->d_scalers;
@@ -185,6 +198,14 @@ static View make_view(Instance *I) {
     v.has_pinv = I->has_pinv;
     v.rescale_every = 16;
     v.pinv = I->pinv;
+    if (slot > 0) {
+        const int ms = model_slot_stride(I->S, I->R);
+        const double *hs = I->h_mslots.data() + (size_t)slot * ms;
+        v.freqs = I->d_mslots + (size_t)slot * ms;
+        v.rate_probs = v.freqs + I->S + I->R;
+        v.pinv = hs[I->S + 2 * I->R];
+        v.has_pinv = hs[I->S + 2 * I->R + 1] != 0.0;
+    }
     return v;
 }
 
@@ -557,6 +578,7 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         {(void **)&I->d_gsync, sizeof(GridSync)},
         {(void **)&I->d_sums2, (size_t)2 * 3 * kMaxScoreBlocks * sizeof(double)},
         {(void **)&I->d_tctab, (I->mixed && I->S != 4) ? kTcTableBytes : (size_t)16},
+        {(void **)&I->d_mslots, (size_t)I->neigen * model_slot_stride(I->S, I->R) * sizeof(double)},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, a.n) != cudaSuccess) {
@@ -569,6 +591,21 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         }
         I->bytes += (long long)a.n;
         cudaMemsetAsync(*a.p, 0, a.n, I->stream);
+    }
+    {
+        // model slots: unit rates and weights 1/R, uniform frequencies, no pinv
+        const int ms = model_slot_stride(I->S, I->R);
+        I->h_mslots.assign((size_t)I->neigen * ms, 0.0);
+        for (int e = 0; e < I->neigen; e++) {
+            double *sl = I->h_mslots.data() + (size_t)e * ms;
+            for (int i = 0; i < I->S; i++) sl[i] = 1.0 / I->S;
+            for (int r = 0; r < I->R; r++) {
+                sl[I->S + r] = 1.0;
+                sl[I->S + I->R + r] = 1.0 / I->R;
+            }
+        }
+        cudaMemcpyAsync(I->d_mslots, I->h_mslots.data(), I->h_mslots.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, I->stream);
     }
     if (cudaMallocHost((void **)&I->h_result, 4 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost((void **)&I->h_status, sizeof(int)) != cudaSuccess) {
@@ -621,7 +658,7 @@ int gb_finalize_instance(int instance) {
                     I->d_result, I->d_site_lnl, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
                     I->d_cmds, I->d_pops, I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots,
                     I->d_chunk_sums, I->d_active, I->d_mentries, I->d_coef, I->d_etab, I->d_cscale,
-                    I->d_tctab};
+                    I->d_tctab, I->d_mslots, I->d_multi, I->d_eq, I->d_epi, I->d_ejobs, I->d_esw};
     if (I->bgraph_exec) cudaGraphExecDestroy(I->bgraph_exec);
     if (I->bgraph) cudaGraphDestroy(I->bgraph);
     for (void *p : ptrs)
@@ -665,6 +702,17 @@ static int upload_patterns(Instance *I) {
 
 // precision form: patterns with count >= kHeavyCount go first (largest counts
 // first if they exceed the FP64 segment), everything else keeps its order
+// write column [off, off + n) of every model slot (or of slot `only`) and upload the table
+static int set_slot_columns(Instance *I, int off, int n, const double *vals, int only = -1) {
+    const int ms = model_slot_stride(I->S, I->R);
+    for (int e = 0; e < I->neigen; e++)
+        if (only < 0 || e == only) std::memcpy(I->h_mslots.data() + (size_t)e * ms + off, vals, n * sizeof(double));
+    GB_CUDA(cudaMemcpyAsync(I->d_mslots, I->h_mslots.data(), I->h_mslots.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    return GB_SUCCESS;
+}
+
 static void make_permutation(Instance *I) {
     std::vector<int> heavy, light;
     for (int q = 0; q < I->npat; q++) (I->h_counts[q] >= kHeavyCount ? heavy : light).push_back(q);
@@ -738,7 +786,7 @@ int gb_set_state_frequencies(int instance, const double *freqs) {
     cudaSetDevice(I->device);
     GB_CUDA(cudaMemcpyAsync(I->d_freqs, freqs, I->S * sizeof(double), cudaMemcpyHostToDevice, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
-    return GB_SUCCESS;
+    return set_slot_columns(I, 0, I->S, freqs);
 }
 
 int gb_set_category_rates(int instance, const double *rates) {
@@ -749,7 +797,7 @@ int gb_set_category_rates(int instance, const double *rates) {
     I->h_rates.assign(rates, rates + I->R);
     GB_CUDA(cudaMemcpyAsync(I->d_rates, rates, I->R * sizeof(double), cudaMemcpyHostToDevice, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
-    return GB_SUCCESS;
+    return set_slot_columns(I, I->S, I->R, rates);
 }
 
 int gb_set_category_weights(int instance, const double *weights) {
@@ -759,7 +807,7 @@ int gb_set_category_weights(int instance, const double *weights) {
     cudaSetDevice(I->device);
     GB_CUDA(cudaMemcpyAsync(I->d_rprobs, weights, I->R * sizeof(double), cudaMemcpyHostToDevice, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
-    return GB_SUCCESS;
+    return set_slot_columns(I, I->S + I->R, I->R, weights);
 }
 
 int gb_set_invariant_sites(int instance, double pinv, int hasPinv) {
@@ -769,7 +817,39 @@ int gb_set_invariant_sites(int instance, double pinv, int hasPinv) {
     if (!(pinv >= 0.0 && pinv < 1.0)) return GB_ERROR_OUT_OF_RANGE;
     I->pinv = pinv;
     I->has_pinv = hasPinv ? 1 : 0;
-    return GB_SUCCESS;
+    cudaSetDevice(I->device);
+    const double pv[2] = {pinv, hasPinv ? 1.0 : 0.0};
+    return set_slot_columns(I, I->S + 2 * I->R, 2, pv);
+}
+
+// One model slot (the parameters read with eigen index eigenIndex): state
+// frequencies, category rates and weights, invariant sites.  Slot 0 is also
+// the instance-wide model of the kernels that take no eigen index; the other
+// slots are left as they are.
+int gb_set_model_slot(int instance, int eigenIndex, const double *freqs, const double *rates,
+                      const double *weights, double pinv, int hasPinv) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (eigenIndex < 0 || eigenIndex >= I->neigen || !freqs || !rates || !weights || !(pinv >= 0.0 && pinv < 1.0))
+        return GB_ERROR_OUT_OF_RANGE;
+    I->version++;
+    cudaSetDevice(I->device);
+    const int S = I->S, R = I->R, ms = model_slot_stride(S, R);
+    if (eigenIndex == 0) {
+        I->h_rates.assign(rates, rates + R);
+        I->pinv = pinv;
+        I->has_pinv = hasPinv ? 1 : 0;
+        GB_CUDA(cudaMemcpyAsync(I->d_freqs, freqs, S * sizeof(double), cudaMemcpyHostToDevice, I->stream));
+        GB_CUDA(cudaMemcpyAsync(I->d_rates, rates, R * sizeof(double), cudaMemcpyHostToDevice, I->stream));
+        GB_CUDA(cudaMemcpyAsync(I->d_rprobs, weights, R * sizeof(double), cudaMemcpyHostToDevice, I->stream));
+    }
+    double *sl = I->h_mslots.data() + (size_t)eigenIndex * ms;
+    std::memcpy(sl, freqs, S * sizeof(double));
+    std::memcpy(sl + S, rates, R * sizeof(double));
+    std::memcpy(sl + S + R, weights, R * sizeof(double));
+    sl[S + 2 * R] = pinv;
+    sl[S + 2 * R + 1] = hasPinv ? 1.0 : 0.0;
+    return set_slot_columns(I, 0, ms, sl, eigenIndex);
 }
 
 int gb_set_eigen_decomposition(int instance, int eigenIndex, const double *U, const double *Uinv,
@@ -810,8 +890,7 @@ int gb_update_transition_matrices(int instance, const gb_transmat_operation *ops
         }
         const size_t smem = pmat_smem_bytes(I->S, I->R);
         k_pmats<<<dim3(T.n, pmat_chunks(I->S, I->R)), kThreads, smem, I->stream>>>(
-            I->d_eigen, I->eig_stride(), I->S, I->R, I->d_rates, I->pinv, I->has_pinv, T, I->d_mats,
-            I->mat_stride());
+            I->d_eigen, I->eig_stride(), I->S, I->R, I->d_mslots, T, I->d_mats, I->mat_stride());
         int rc = check_launch(I);
         if (rc) return rc;
     }
@@ -922,16 +1001,17 @@ int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int
     return GB_SUCCESS;
 }
 
-static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, bool sync) {
+// enqueue one edge evaluation under model slot `slot`; its (lnL, d1, d2) go to dres
+static int edge_enqueue(Instance *I, const gb_scoring_operation *op, int slot, double *dres) {
     const int nt = I->ntip;
     const int pb = op->childClaIndex1 - nt;
     const int cb = op->childClaIndex2;
     if (pb < 0 || pb >= I->nbuf || cb < 0 || cb >= nt + I->nbuf || op->transMatIndex < 0 ||
-        op->transMatIndex >= I->nmat)
+        op->transMatIndex >= I->nmat || slot < 0 || slot >= I->neigen)
         return GB_ERROR_OUT_OF_RANGE;
     const int tip = cb < nt;
     const int cidx = tip ? cb : cb - nt;
-    View v = make_view(I);
+    View v = make_view(I, slot);
     const bool D = op->derivatives != 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (I->timing) {
@@ -963,7 +1043,7 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
     }
     int rc = check_launch(I);
     if (rc) return rc;
-    k_reduce3<<<1, kThreads, 0, I->stream>>>(I->d_block_sums, nblocks, I->d_result);
+    k_reduce3<<<1, kThreads, 0, I->stream>>>(I->d_block_sums, nblocks, dres);
     rc = check_launch(I);
     if (rc) return rc;
     if (I->timing) {
@@ -971,13 +1051,11 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
         I->ev_edge.emplace_back(e0, e1);
     }
     I->site_valid = true;
-    if (!sync) return GB_SUCCESS;
-    GB_CUDA(cudaMemcpyAsync(I->h_result, I->d_result, 3 * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
-    GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
-    GB_CUDA(cudaStreamSynchronize(I->stream));
-    out[0] = I->h_result[0];
-    out[1] = D ? I->h_result[1] : 0.0;
-    out[2] = D ? I->h_result[2] : 0.0;
+    return GB_SUCCESS;
+}
+
+// status word of the work enqueued so far (read after a stream synchronisation)
+static int edge_status(Instance *I) {
     if (*I->h_status & kStatusTcRange) {
         // a product maximum below the tensor-core path's range: the CLAs are
         // recomputed on the CUDA cores (the tree drivers redo the score on
@@ -1005,6 +1083,20 @@ static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, b
         GB_CUDA(cudaStreamSynchronize(I->stream));
         return GB_ERROR_RESCALE_RETRY;
     }
+    return GB_SUCCESS;
+}
+
+static int edge_impl(Instance *I, const gb_scoring_operation *op, double *out, bool sync) {
+    int rc = edge_enqueue(I, op, 0, I->d_result);
+    if (rc || !sync) return rc;
+    const bool D = op->derivatives != 0;
+    GB_CUDA(cudaMemcpyAsync(I->h_result, I->d_result, 3 * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    out[0] = I->h_result[0];
+    out[1] = D ? I->h_result[1] : 0.0;
+    out[2] = D ? I->h_result[2] : 0.0;
+    if ((rc = edge_status(I))) return rc;
     if (!std::isfinite(out[0])) return GB_ERROR_FLOATING_POINT;
     return GB_SUCCESS;
 }
@@ -1015,6 +1107,44 @@ int gb_calculate_edge(int instance, const gb_scoring_operation *op, double *out)
     if (!op || !out) return GB_ERROR_OUT_OF_RANGE;
     cudaSetDevice(I->device);
     return edge_impl(I, op, out, true);
+}
+
+// count edge evaluations, edge k under model slot modelSlots[k] (all slot 0
+// when modelSlots is NULL), with one synchronisation; out[3k .. 3k+2]
+int gb_calculate_edges(int instance, const gb_scoring_operation *ops, const int *modelSlots, int count,
+                       double *out) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!ops || !out || count < 1) return GB_ERROR_OUT_OF_RANGE;
+    cudaSetDevice(I->device);
+    if ((size_t)count * 3 > I->cap_multi) {
+        cudaFree(I->d_multi);
+        I->d_multi = nullptr;
+        I->cap_multi = 0;
+        if (cudaMalloc(&I->d_multi, (size_t)count * 3 * sizeof(double)) != cudaSuccess) {
+            g_last_error = "gb_calculate_edges: cudaMalloc failed";
+            return GB_ERROR_OUT_OF_MEMORY;
+        }
+        I->cap_multi = (size_t)count * 3;
+    }
+    for (int k = 0; k < count; k++) {
+        int rc = edge_enqueue(I, ops + k, modelSlots ? modelSlots[k] : 0, I->d_multi + 3 * k);
+        if (rc) return rc;
+    }
+    std::vector<double> res((size_t)count * 3);
+    GB_CUDA(cudaMemcpyAsync(res.data(), I->d_multi, res.size() * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaMemcpyAsync(I->h_status, I->d_status, sizeof(int), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    int rc = edge_status(I);
+    if (rc) return rc;
+    for (int k = 0; k < count; k++) {
+        const bool D = ops[k].derivatives != 0;
+        out[3 * k] = res[3 * k];
+        out[3 * k + 1] = D ? res[3 * k + 1] : 0.0;
+        out[3 * k + 2] = D ? res[3 * k + 2] : 0.0;
+        if (!std::isfinite(out[3 * k])) return GB_ERROR_FLOATING_POINT;
+    }
+    return GB_SUCCESS;
 }
 
 int gb_get_site_log_likelihoods(int instance, double *out) {
@@ -1098,6 +1228,15 @@ int gb_get_partials_pool(int instance, void **devicePtr, long long *bytes) {
     if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
     if (devicePtr) *devicePtr = I->d_partials;
     if (bytes) *bytes = (long long)I->nbuf * I->cla_bytes;
+    return GB_SUCCESS;
+}
+
+int gb_get_instance_capacity(int instance, int *out) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    out[0] = I->nbuf;
+    out[1] = I->nmat;
+    out[2] = I->neigen;
     return GB_SUCCESS;
 }
 
@@ -2198,23 +2337,29 @@ int gb_set_eigen_from_rate_matrices(int instance, int count, const int *eigenInd
             if (!(pi[c * S + i] > 0.0)) return GB_ERROR_OUT_OF_RANGE;  // D^1/2 needs positive frequencies
     }
     cudaSetDevice(I->device);
-    double *dQ = nullptr, *dpi = nullptr;
-    EigenJob *djobs = nullptr;
-    int *dsw = nullptr;
-    auto release = [&]() {
-        cudaFree(dQ);
-        cudaFree(dpi);
-        cudaFree(djobs);
-        cudaFree(dsw);
-    };
-    if (cudaMalloc(&dQ, (size_t)count * S * S * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&dpi, (size_t)count * S * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&djobs, (size_t)count * sizeof(EigenJob)) != cudaSuccess ||
-        cudaMalloc(&dsw, (size_t)count * sizeof(int)) != cudaSuccess) {
-        release();
-        g_last_error = "gb_set_eigen_from_rate_matrices: cudaMalloc failed";
-        return GB_ERROR_OUT_OF_MEMORY;
+    if (count > I->cap_eig) {
+        // the previous scratch may still be read by queued work
+        GB_CUDA(cudaStreamSynchronize(I->stream));
+        cudaFree(I->d_eq);
+        cudaFree(I->d_epi);
+        cudaFree(I->d_ejobs);
+        cudaFree(I->d_esw);
+        I->d_eq = I->d_epi = nullptr;
+        I->d_ejobs = nullptr;
+        I->d_esw = nullptr;
+        I->cap_eig = 0;
+        if (cudaMalloc(&I->d_eq, (size_t)count * S * S * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&I->d_epi, (size_t)count * S * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&I->d_ejobs, (size_t)count * sizeof(EigenJob)) != cudaSuccess ||
+            cudaMalloc(&I->d_esw, (size_t)count * sizeof(int)) != cudaSuccess) {
+            g_last_error = "gb_set_eigen_from_rate_matrices: cudaMalloc failed";
+            return GB_ERROR_OUT_OF_MEMORY;
+        }
+        I->cap_eig = count;
     }
+    double *dQ = I->d_eq, *dpi = I->d_epi;
+    EigenJob *djobs = I->d_ejobs;
+    int *dsw = I->d_esw;
     std::vector<EigenJob> jobs(count);
     for (int c = 0; c < count; c++) {
         jobs[c].Q = dQ + (size_t)c * S * S;
@@ -2236,7 +2381,6 @@ int gb_set_eigen_from_rate_matrices(int instance, int count, const int *eigenInd
     if (!rc && cudaMemcpyAsync(sw.data(), dsw, (size_t)count * sizeof(int), cudaMemcpyDeviceToHost, I->stream))
         rc = GB_ERROR_GENERAL;
     if (cudaStreamSynchronize(I->stream) != cudaSuccess) rc = GB_ERROR_GENERAL;
-    release();
     if (rc) return rc;
     if (sweepsOut)
         for (int c = 0; c < count; c++) sweepsOut[c] = sw[c];

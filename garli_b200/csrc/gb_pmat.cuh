@@ -83,12 +83,19 @@ __device__ __forceinline__ void pmat_body(const double *eig, long long eig_strid
     }
 }
 
-// grid (matrices, pmat_chunks(S, R))
+// Model slot table: per eigen index, [freqs (S) | category rates (R) |
+// category weights (R) | pinv | has_pinv], model_slot_stride(S, R) doubles.
+__host__ __device__ constexpr int model_slot_stride(int S, int R) { return S + 2 * R + 2; }
+
+// grid (matrices, pmat_chunks(S, R)); each matrix takes the rates and pinv of
+// its eigen index's model slot
 __global__ void __launch_bounds__(kThreads) k_pmats(const double *eig, long long eig_stride, int S, int R,
-                                                    const double *rates, double pinv, int has_pinv,
-                                                    TransOps ops, double *mats, long long mat_stride) {
-    pmat_body(eig, eig_stride, S, R, rates, pinv, has_pinv, ops.op[blockIdx.x], mats, mat_stride, blockIdx.y,
-              gridDim.y);
+                                                    const double *mslots, TransOps ops, double *mats,
+                                                    long long mat_stride) {
+    const TransOp op = ops.op[blockIdx.x];
+    const double *slot = mslots + (long long)op.eigen * model_slot_stride(S, R);
+    pmat_body(eig, eig_stride, S, R, slot + S, slot[S + 2 * R], slot[S + 2 * R + 1] != 0.0 ? 1 : 0, op, mats,
+              mat_stride, blockIdx.y, gridDim.y);
 }
 
 // P(t), dP/dt, d2P/dt2 of one matrix whose branch length lives on the device

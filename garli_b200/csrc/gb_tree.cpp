@@ -14,6 +14,7 @@
 //   * Tree::Score's rescale retry loop (tree.cpp:4003-4100);
 //   * NewtonRaphsonOptimizeBranchLength (optimization.cpp:1359-1971) and
 //     OptimizeAllBranches / RecursivelyOptimizeBranches (optimization.cpp:97, :1042).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -415,9 +416,109 @@ int optimize_all_device(Tree &t, double prec, double *out) {
     }
 }
 
+// Tree::Score after MakeAllNodesDirty under count models at once (one
+// SetAndEvaluateParameter per model, optimization.cpp:244-268): model k reads
+// eigen / model slot slots[k], its P(t) in matrices (k+1)*nnodes + node and
+// its Down CLAs in buffers past the tree's own 3 per internal node.  The
+// operations of all models go to the engine as one levelled list, the root
+// edges as one gb_calculate_edges call; the tree's own CLAs and P(t) are not
+// touched.  The CLAs scored are those of the root request at node 0 with
+// every holder dirty (root_request): Down(0) against the middle child's Down.
+int score_models(Tree &t, int count, const int *slots, double *lnl) {
+    int cap[3];
+    int rc = gb_get_instance_capacity(t.inst, cap);
+    if (rc) return rc;
+    const int nint = t.ntax - 2;
+    if (cap[0] < 3 * nint + count * nint || cap[1] < (count + 1) * t.nnodes) return GB_ERROR_OUT_OF_RANGE;
+    for (int k = 0; k < count; k++)
+        if (slots[k] < 0 || slots[k] >= cap[2]) return GB_ERROR_OUT_OF_RANGE;
+    auto kbuf = [&](int k, int nd) { return t.ntax + 3 * nint + k * nint + (nd == 0 ? 0 : nd - t.ntax); };
+    auto kmat = [&](int k, int nd) { return (k + 1) * t.nnodes + nd; };
+    // dependency level of each internal node's Down holder (tips: 0), as accumulate() numbers them
+    std::vector<int> lvl(t.nnodes, 0), post;
+    std::vector<int> stack{0};
+    while (!stack.empty()) {
+        const int nd = stack.back();
+        stack.pop_back();
+        post.push_back(nd);
+        for (int c = t.left[nd]; c >= 0; c = t.next[c])
+            if (t.internal(c)) stack.push_back(c);
+    }
+    for (int i = (int)post.size() - 1; i >= 0; i--) {
+        const int nd = post[i];
+        const Deps d = deps_of(t, nd, DOWN);
+        lvl[nd] = std::max(d.w1 >= 0 ? lvl[d.n1] : 0, d.w2 >= 0 ? lvl[d.n2] : 0) + 1;
+    }
+    const int mid = t.next[t.left[0]];
+    for (;;) {
+        std::vector<gb_transmat_operation> tops;
+        std::vector<gb_cla_operation> ops;
+        std::vector<gb_scoring_operation> sops(count);
+        for (int k = 0; k < count; k++) {
+            for (int nd = 1; nd < t.nnodes; nd++) {
+                gb_transmat_operation o;
+                o.destTransMatIndex = kmat(k, nd);
+                o.edgeLength = t.dlen[nd];
+                o.eigenIndex = slots[k];
+                o.calcDerivs = 0;
+                tops.push_back(o);
+            }
+            for (int nd : post) {
+                const Deps d = deps_of(t, nd, DOWN);
+                gb_cla_operation op;
+                op.destClaIndex = kbuf(k, nd);
+                op.childClaIndex1 = d.w1 >= 0 ? kbuf(k, d.n1) : t.tipbuf(d.n1);
+                op.childClaIndex2 = d.w2 >= 0 ? kbuf(k, d.n2) : t.tipbuf(d.n2);
+                op.transMatIndex1 = kmat(k, d.m1);
+                op.transMatIndex2 = kmat(k, d.m2);
+                op.opDepLevel = lvl[nd];
+                ops.push_back(op);
+            }
+            gb_scoring_operation &so = sops[k];
+            so.destClaIndex = -1;
+            so.childClaIndex1 = kbuf(k, 0);
+            so.childClaIndex2 = t.internal(mid) ? kbuf(k, mid) : t.tipbuf(mid);
+            so.transMatIndex = kmat(k, mid);
+            so.derivatives = 0;
+        }
+        if ((rc = gb_update_transition_matrices(t.inst, tops.data(), (int)tops.size()))) return rc;
+        if ((rc = gb_update_partials(t.inst, ops.data(), (int)ops.size(), t.rescaleEvery))) return rc;
+        std::vector<double> out(3 * (size_t)count);
+        rc = gb_calculate_edges(t.inst, sops.data(), slots, count, out.data());
+        t.nOps += (long long)ops.size();
+        t.nPatUpdates += (long long)ops.size() * t.npat;
+        t.nEdge += count;
+        if (rc == GB_ERROR_RESCALE_RETRY) {
+            // Tree::Score's retry (tree.cpp:4077-4090)
+            t.nRetries++;
+            make_all_dirty(t);
+            t.rescaleEvery -= 2;
+            if (t.rescaleEvery < 2) return GB_ERROR_FLOATING_POINT;
+            continue;
+        }
+        if (rc) return rc;
+        for (int k = 0; k < count; k++) lnl[k] = out[3 * k];
+        t.nScores += count;
+        return GB_SUCCESS;
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+int gbt_score_models(int tree, int count, const int *eigenIndices, double *lnl) {
+    Tree *t = get(tree);
+    if (!t) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (count < 1 || !eigenIndices || !lnl) return GB_ERROR_OUT_OF_RANGE;
+    return score_models(*t, count, eigenIndices, lnl);
+}
+
+int gbt_get_instance(int tree) {
+    Tree *t = get(tree);
+    if (!t) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    return t->inst;
+}
 
 int gbt_create(int instance, int ntax, const int *child3, const double *dlen) {
     if (ntax < 3 || !child3 || !dlen) return GB_ERROR_OUT_OF_RANGE;

@@ -54,6 +54,13 @@ class ScoringOperation(C.Structure):
                 ("transMatIndex", C.c_int), ("derivatives", C.c_int)]
 
 
+class ModelParams(C.Structure):
+    """gb_model_params: GARLI's Model parameters of one tree (model.h)."""
+    _fields_ = [("kind", C.c_int), ("stateCount", C.c_int), ("categoryCount", C.c_int), ("nst", C.c_int),
+                ("hasPinv", C.c_int), ("alpha", C.c_double), ("pinv", C.c_double), ("maxPinv", C.c_double),
+                ("omega", C.c_double), ("rel", C.c_double * 6), ("pi", C.c_double * 64)]
+
+
 class InstanceDetails(C.Structure):
     _fields_ = [("resourceNumber", C.c_int), ("flags", C.c_long), ("paddedPatterns", C.c_int),
                 ("deviceBytes", C.c_longlong), ("deviceName", C.c_char * 64)]
@@ -142,6 +149,22 @@ SIGNATURES = {
     "gbt_set_rescale_every": (C.c_int, [C.c_int, C.c_int]),
     "gbt_get_counters": (C.c_int, [C.c_int, _LL]),
     "gbt_cla_buffer": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "gbt_score_models": (C.c_int, [C.c_int, C.c_int, _I, _D]),
+    "gbt_get_instance": (C.c_int, [C.c_int]),
+    "gb_set_model_slot": (C.c_int, [C.c_int, C.c_int, _D, _D, _D, C.c_double, C.c_int]),
+    "gb_calculate_edges": (C.c_int, [C.c_int, C.POINTER(ScoringOperation), _I, C.c_int, _D]),
+    "gb_get_instance_capacity": (C.c_int, [C.c_int, _I]),
+    "gbo_create": (C.c_int, [C.c_int, C.POINTER(ModelParams), _D]),
+    "gbo_destroy": (C.c_int, [C.c_int]),
+    "gbo_get_model": (C.c_int, [C.c_int, C.POINTER(ModelParams)]),
+    "gbo_set_model": (C.c_int, [C.c_int, C.POINTER(ModelParams)]),
+    "gbo_optimize_parameter": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         _D]),
+    "gbo_optimize_model": (C.c_int, [C.c_int, C.c_int, C.c_double, _D]),
+    "gbo_final_optimization": (C.c_int, [C.c_int, C.c_double, C.c_int, C.c_int, _D]),
+    "gbo_set_batching": (C.c_int, [C.c_int, C.c_int]),
+    "gbo_get_counters": (C.c_int, [C.c_int, _LL]),
+    "gbo_get_trace": (C.c_int, [C.c_int, _D, _D, C.c_int, _D]),
 }
 
 
@@ -378,6 +401,17 @@ class Instance:
     def set_tensor_cores(self, on: bool):
         _chk(lib().gb_set_tensor_cores(self.h, int(on)), "gb_set_tensor_cores")
 
+    def set_model_slot(self, slot, pi, rates, weights, pinv=0.0, has_pinv=False):
+        """Frequencies, category rates / weights and pinv read with eigen index ``slot``."""
+        _chk(lib().gb_set_model_slot(self.h, int(slot), _p(_f64(pi), C.c_double), _p(_f64(rates), C.c_double),
+                                     _p(_f64(weights), C.c_double), float(pinv), int(has_pinv)),
+             "gb_set_model_slot")
+
+    def capacity(self) -> tuple:
+        out = np.zeros(3, dtype=np.int32)
+        _chk(lib().gb_get_instance_capacity(self.h, _p(out, C.c_int)), "gb_get_instance_capacity")
+        return int(out[0]), int(out[1]), int(out[2])
+
     def set_pass_mode(self, persistent: bool):
         _chk(lib().gb_set_pass_mode(self.h, int(persistent)), "gb_set_pass_mode")
 
@@ -451,6 +485,120 @@ class Tree:
 
     def cla_buffer(self, node, which) -> int:
         return lib().gbt_cla_buffer(self.h, node, which)
+
+
+    def score_models(self, slots) -> np.ndarray:
+        """Full rescores of the tree under the models in eigen / model slots ``slots``."""
+        sl = _i32(slots)
+        out = np.zeros(len(sl))
+        _chk(lib().gbt_score_models(self.h, len(sl), _p(sl, C.c_int), _p(out, C.c_double)), "gbt_score_models")
+        return out
+
+
+# GB_MODEL_*, GB_PARAM_*, GB_OPT_* (include/garli_b200.h)
+MODEL_NUCLEOTIDE, MODEL_AMINO_ACID, MODEL_CODON = 0, 1, 2
+PARAM_ALPHA, PARAM_PINV, PARAM_STATE_FREQ, PARAM_REL_RATE, PARAM_OMEGA = 0, 1, 2, 3, 4
+OPT_ALPHA, OPT_PINV, OPT_FREQS, OPT_RATES, OPT_OMEGA = 1, 2, 4, 8, 16
+
+
+def model_params(kind, pi, rel=None, alpha=0.5, ncat=1, pinv=None, max_pinv=0.0, omega=1.0, nst=6) -> ModelParams:
+    """gb_model_params from plain values (pinv None: no invariant-sites class)."""
+    m = ModelParams()
+    m.kind = kind
+    m.stateCount = len(pi)
+    m.categoryCount = ncat
+    m.nst = nst
+    m.hasPinv = 0 if pinv is None else 1
+    m.alpha = alpha
+    m.pinv = 0.0 if pinv is None else float(pinv)
+    m.maxPinv = max_pinv
+    m.omega = omega
+    for i, v in enumerate(rel if rel is not None else [1.0] * 6):
+        m.rel[i] = float(v)
+    for i, v in enumerate(pi):
+        m.pi[i] = float(v)
+    return m
+
+
+class ModelOptimizer:
+    """GARLI's model-parameter optimisation of one tree (gbo_* in the ABI)."""
+
+    def __init__(self, tree: "Tree", params: ModelParams, exch=None):
+        self.tree = tree
+        ex = None if exch is None else _f64(exch)
+        h = lib().gbo_create(tree.h, C.byref(params), None if ex is None else _p(ex, C.c_double))
+        _chk(h, "gbo_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", -1) >= 0:
+            lib().gbo_destroy(self.h)
+            self.h = -1
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> ModelParams:
+        m = ModelParams()
+        _chk(lib().gbo_get_model(self.h, C.byref(m)), "gbo_get_model")
+        return m
+
+    def set_params(self, m: ModelParams):
+        _chk(lib().gbo_set_model(self.h, C.byref(m)), "gbo_set_model")
+
+    def optimize_parameter(self, param, which, precision, low, high, target_digits=9.0):
+        """OptimizeBoundedParameter: (improvement, final lnL)."""
+        out = np.zeros(2)
+        _chk(lib().gbo_optimize_parameter(self.h, param, which, float(precision), float(low), float(high),
+                                          float(target_digits), _p(out, C.c_double)), "gbo_optimize_parameter")
+        return float(out[0]), float(out[1])
+
+    def optimize_model(self, mask, precision) -> np.ndarray:
+        out = np.zeros(5)
+        _chk(lib().gbo_optimize_model(self.h, int(mask), float(precision), _p(out, C.c_double)),
+             "gbo_optimize_model")
+        return out
+
+    def final_optimization(self, branch_precision=0.01, mask=31, max_passes=0):
+        """BetterFinalOptimization: (final lnL, passes, model evaluations)."""
+        out = np.zeros(3)
+        _chk(lib().gbo_final_optimization(self.h, float(branch_precision), int(mask), int(max_passes),
+                                          _p(out, C.c_double)), "gbo_final_optimization")
+        return float(out[0]), int(out[1]), int(out[2])
+
+    def set_batching(self, depth: int):
+        _chk(lib().gbo_set_batching(self.h, int(depth)), "gbo_set_batching")
+
+    def trace(self):
+        """(initial lnL, values, scores) of the last OptimizeBoundedParameter call."""
+        ini = C.c_double()
+        n = _chk(lib().gbo_get_trace(self.h, None, None, 0, C.byref(ini)), "gbo_get_trace")
+        v, sc = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        _chk(lib().gbo_get_trace(self.h, _p(v, C.c_double), _p(sc, C.c_double), n, None), "gbo_get_trace")
+        return ini.value, v[:n], sc[:n]
+
+    def counters(self) -> dict:
+        out = np.zeros(3, dtype=np.int64)
+        _chk(lib().gbo_get_counters(self.h, _p(out, C.c_longlong)), "gbo_get_counters")
+        return {"evaluations": int(out[0]), "models_scored": int(out[1]), "score_calls": int(out[2])}
+
+
+def model_engine(pd, child3, dlen, params: ModelParams, kmax=8, exch=None, device=0):
+    """Instance, Tree and ModelOptimizer for model-parameter optimisation of one
+    tree: room for kmax candidate models per batched rescore."""
+    ntax = pd.ntax
+    nnodes = 2 * ntax - 2
+    nint = ntax - 2
+    inst = Instance(ntax, (3 + kmax) * nint, pd.nstates, pd.npat, params.categoryCount, (kmax + 1) * nnodes,
+                    neigen=kmax + 1, device=device)
+    inst.set_data(pd)
+    tree = Tree(inst, child3, dlen)
+    opt = ModelOptimizer(tree, params, exch)
+    return inst, tree, opt
 
 
 def tree_engine(pd, child3, dlen, model: Model, device=0, mixed=False):

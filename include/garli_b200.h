@@ -117,6 +117,15 @@ int gb_set_invariant_sites(int instance, double pinv, int hasPinv);
  * multiplied by GARLI's blen_multiplier (model.cpp:845) */
 int gb_set_eigen_decomposition(int instance, int eigenIndex, const double *eigenVectors,
                                const double *inverseEigenVectors, const double *eigenValues);
+/* Model slots: eigen index e also selects the state frequencies, category
+ * rates, category weights and invariant-sites term that P(t) (transition
+ * matrix operations with eigenIndex e) and edge evaluations under slot e use.
+ * The four instance-wide setters above write every slot; this one writes
+ * slot eigenIndex only (slot 0 is also the instance-wide model).  One tree
+ * scored under several models at once (optimization.cpp:244-268, a Model per
+ * candidate parameter value) keeps each model in its own slot. */
+int gb_set_model_slot(int instance, int eigenIndex, const double *freqs, const double *rates,
+                      const double *weights, double pinv, int hasPinv);
 
 /* ---- operations ---- */
 /* Model::CalcEigenStuff (model.cpp:827-856) on the device, FP64, one CTA per
@@ -146,6 +155,12 @@ int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int
 /* beagleCalculateEdgeLogLikelihoods (subsetcalculationmanager.cpp:765-901):
  * returns lnL and, when op->derivatives, d1 and d2 in outLnL[0..2]. */
 int gb_calculate_edge(int instance, const gb_scoring_operation *op, double *out);
+/* count edge evaluations with one synchronisation: edge k under model slot
+ * modelSlots[k] (NULL: slot 0 for all); out[3k], out[3k+1], out[3k+2] = lnL,
+ * d1, d2 of edge k.  A rescale-retry or range condition of any edge is
+ * reported for the whole call. */
+int gb_calculate_edges(int instance, const gb_scoring_operation *ops, const int *modelSlots, int count,
+                       double *out);
 /* beagleGetSiteLogLikelihoods of the last gb_calculate_edge (unscaled per pattern) */
 int gb_get_site_log_likelihoods(int instance, double *out);
 /* debug read-back (beagleGetPartials / beagleGetScaleFactors); CLA layout
@@ -157,6 +172,8 @@ int gb_get_transition_matrix(int instance, int matrixIndex, int which, double *o
 int gb_get_rescale_rank(int instance, int bufferIndex);
 /* raw device pointer and size of the CLA pool (for peer copies / profiling) */
 int gb_get_partials_pool(int instance, void **devicePtr, long long *bytes);
+/* out[0..2] = partialsBufferCount, matrixBufferCount, eigenBufferCount */
+int gb_get_instance_capacity(int instance, int *out);
 /* out[0..4] = tipCount, partialsBufferCount, stateCount, categoryCount, patternCount */
 int gb_get_instance_shape(int instance, int *out);
 /* number of engine kernels launched since the instance was created */
@@ -402,6 +419,73 @@ int gbt_set_rescale_every(int tree, int every);
 int gbt_get_counters(int tree, long long *out5);
 /* CLA buffer index currently holding (node, which) with which 0=Down 1=UL 2=UR; -1 if dirty */
 int gbt_cla_buffer(int tree, int node, int which);
+/* Tree::Score at root 0 after MakeAllNodesDirty under count models at once
+ * (one SetAndEvaluateParameter each, optimization.cpp:244-268): model k uses
+ * eigen / model slot eigenIndices[k], matrices (k+1)*nnodes + node and CLA
+ * buffers 3*(ntax-2) + k*(ntax-2) + j past the tip buffers; the tree's own
+ * CLAs and P(t) stay as they are.  Needs partialsBufferCount >=
+ * (3 + count)*(ntax-2) and matrixBufferCount >= (count+1)*nnodes.  lnl[k] =
+ * the score under model k; a rescale retry redoes all (tree.cpp:4077-4090). */
+int gbt_score_models(int tree, int count, const int *eigenIndices, double *lnl);
+/* engine instance the tree runs on */
+int gbt_get_instance(int tree);
+
+/* ---- model-parameter optimisation (optimization.cpp:244-776, tree.cpp:7160-7410,
+ * population.cpp:2566-2790) ----
+ * GARLI's Model parameters of one tree, their setters and
+ * Tree::OptimizeBoundedParameter.  Every candidate parameter value is a whole
+ * model (Q, eigen system, discrete-gamma rates, pinv weights) scored by a full
+ * rescore; evaluation points whose values are fixed before their scores are
+ * needed (the bump, the first pair of points, the next pass's pair beside each
+ * proposed value) are scored together through gbt_score_models, eigen systems
+ * through gb_set_eigen_from_rate_matrices, and the decisions are GARLI's own in
+ * GARLI's order. */
+enum { GB_MODEL_NUCLEOTIDE = 0, GB_MODEL_AMINO_ACID = 1, GB_MODEL_CODON = 2 };
+enum { GB_PARAM_ALPHA = 0, GB_PARAM_PINV = 1, GB_PARAM_STATE_FREQ = 2, GB_PARAM_REL_RATE = 3, GB_PARAM_OMEGA = 4 };
+enum { GB_OPT_ALPHA = 1, GB_OPT_PINV = 2, GB_OPT_FREQS = 4, GB_OPT_RATES = 8, GB_OPT_OMEGA = 16 };
+typedef struct {
+    int kind;          /* GB_MODEL_* */
+    int stateCount;    /* 4, 20 or 61 */
+    int categoryCount; /* discrete-gamma categories (1: no rate heterogeneity) */
+    int nst;           /* nucleotide / codon rate classes: 1, 2 (transition / transversion) or 6 */
+    int hasPinv;
+    double alpha, pinv;
+    double maxPinv;    /* Model::maxPropInvar (model.cpp:1649): constant / all sites */
+    double omega;      /* codon dN/dS */
+    double rel[6];     /* AC AG AT CG CT GT, GT = 1 (model.h:1518-1531) */
+    double pi[64];     /* state frequencies, stateCount used */
+} gb_model_params;
+/* optimiser for the model of tree; aaExchangeabilities (190, amino acids
+ * only) stay fixed.  Installs the model as the tree's model (slot 0). */
+int gbo_create(int tree, const gb_model_params *model, const double *aaExchangeabilities);
+int gbo_destroy(int opt);
+int gbo_get_model(int opt, gb_model_params *out);
+int gbo_set_model(int opt, const gb_model_params *model);
+/* Tree::OptimizeBoundedParameter(which, lowBound, highBound, setter,
+ * targetScoreDigits) for parameter GB_PARAM_*; out[0] = lnL - initial lnL,
+ * out[1] = final lnL */
+int gbo_optimize_parameter(int opt, int param, int which, double precision, double lowBound, double highBound,
+                           double targetScoreDigits, double *out);
+/* one pass of Population::BetterFinalOptimization's model part for the
+ * parameters in mask (GB_OPT_*), with GARLI's bounds: alpha
+ * (population.cpp:2702), pinv (:2727), OptimizeEquilibriumFreqs
+ * (tree.cpp:7288), OptimizeRelativeNucRates (tree.cpp:7307), single-class
+ * omega (tree.cpp:7186); out[0..4] = improvement per GB_PARAM_* kind */
+int gbo_optimize_model(int opt, int mask, double precision, double *out5);
+/* Population::BetterFinalOptimization (population.cpp:2566-2790): passes of
+ * OptimizeAllBranches + the parameters in mask until GARLI's exit rule;
+ * out[0] = final lnL, out[1] = passes, out[2] = model evaluations */
+int gbo_final_optimization(int opt, double branchOptPrecision, int mask, int maxPasses, double *out3);
+/* 1 (default): evaluation points known in advance are scored in one batch;
+ * 0: one model per gbt_score_models call, in GARLI's order */
+int gbo_set_batching(int opt, int on);
+/* the evaluations of the last OptimizeBoundedParameter call in GARLI's order
+ * (SetAndEvaluateParameter values and scores, up to capacity) and the score it
+ * started from; returns their number */
+int gbo_get_trace(int opt, double *values, double *scores, int capacity, double *initialScore);
+/* counters: [0] model evaluations GARLI makes, [1] models scored (speculative
+ * ones included), [2] gbt_score_models calls */
+int gbo_get_counters(int opt, long long *out3);
 
 #ifdef __cplusplus
 }

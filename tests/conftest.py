@@ -51,6 +51,25 @@ def fixture_model(fx, mathlib):
                  np.full(R, (1.0 - pinv) / R), pinv, has)
 
 
+def fixture_params(fx, pd):
+    """GARLI's model parameters of a DNA fixture: (kind, pi, rel, alpha, ncat,
+    pinv, maxPinv) with maxPinv = constant sites / all sites (model.cpp:1649)."""
+    m = fx["model"]
+    pi = np.array(m["e"], dtype=np.float64)
+    pi = pi / pi.sum()
+    nconst = int(np.sum(pd.counts[: pd.last_const + 1]))
+    return dict(pi=pi, rel=np.array(m["r"], dtype=np.float64), alpha=m["a"], ncat=m["ncat"], pinv=m["p"],
+                max_pinv=nconst / float(np.sum(pd.counts)))
+
+
+def scoring_test_score(fx, lnl, site_lnl):
+    """The number the reference's scoring test compares with expected.scr
+    (tests/runtests.sh): -lnL + 1/2 sum (w_c - 1) lnL_c over the weighted
+    columns of the test's data file (make_fixtures.wtset_sitelike_extra)."""
+    st = fx["scoring_test"]
+    return -lnl + 0.5 * sum(e * site_lnl[p] for p, e in st["sitelike_extra"])
+
+
 @pytest.fixture(scope="session")
 def has_gpu():
     try:

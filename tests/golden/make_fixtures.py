@@ -74,6 +74,69 @@ def read_start(path):
     return trans, score, params, newick
 
 
+def parse_set(spec, nchar):
+    """1-based character numbers of a NEXUS set list ("1-749 751-1008 1930-.")."""
+    out = []
+    for tok in spec.split():
+        if "-" in tok:
+            a, b = tok.split("-")
+            out.extend(range(int(a), (nchar if b == "." else int(b)) + 1))
+        else:
+            out.append(int(tok))
+    return out
+
+
+def wtset_sitelike_extra(pd, plain_masks):
+    """The scoring tests of n.G4 / n.G5 read z.11x2178.wtset.nex: 2,180 columns
+    with an exset and a compensating integer wtset (assumptions block).  Their
+    check (tests/runtests.sh) halves the sum of column 2 of the sitelikes file:
+    the tree's -lnL plus one -lnL per non-excluded column, written once whatever
+    its weight (Tree::OutputSiteLikelihoods, tree.cpp:5500-5560).  With weights
+    w_c the number compared is therefore -lnL + 1/2 sum_c (w_c - 1) lnL_c.
+    Returns [(pattern index in pd, w_c - 1)] for the columns with w_c != 1,
+    after checking that the weighted columns are the plain matrix's columns
+    plus all-missing ones (so the tree's lnL is the plain data's)."""
+    order, rows = read_nexus_matrix(os.path.join(DATA, "z.11x2178.wtset.nex"))
+    txt = open(os.path.join(DATA, "z.11x2178.wtset.nex")).read()
+    txt = re.sub(r"\[[^\]]*\]", "", txt)
+    nchar = len(rows[order[0]])
+    ex = set(parse_set(re.search(r"exset\s*\*\s*\S+\s*=\s*([^;]*);", txt, re.I).group(1), nchar))
+    w = {}
+    for part in re.search(r"wtset\s*\*\s*\S+\s*=\s*([^;]*);", txt, re.I).group(1).split(","):
+        wt, lst = part.split(":")
+        for c in parse_set(lst, nchar):
+            w[c] = int(wt)
+    porder, prows = read_nexus_matrix(os.path.join(DATA, "z.11x2178.nex"))
+    assert order == porder
+    col = lambda r, o, c: "".join(r[t][c - 1].upper() for t in o)
+    missing = lambda s: all(ch in "N?-" for ch in s)
+    from collections import Counter
+    weighted, plain = Counter(), Counter()
+    for c in range(1, nchar + 1):
+        if c not in ex and not missing(col(rows, order, c)):
+            weighted[col(rows, order, c)] += w.get(c, 1)
+    for c in range(1, len(prows[porder[0]]) + 1):
+        plain[col(prows, porder, c)] += 1
+    assert weighted == plain, "the weighted matrix is not the plain one"
+    # pattern of each plain column, by its tip masks
+    key = {bytes(pd.tips[:, j].tolist()): j for j in range(pd.npat)}
+    extra = []
+    for c in sorted(w):
+        if c in ex or w[c] == 1 or missing(col(rows, order, c)):
+            continue
+        j = next(j for j in range(plain_masks.shape[1]) if col(prows, porder, j + 1) == col(rows, order, c))
+        extra.append([key[bytes(plain_masks[:, j].tolist())], w[c] - 1])
+    return extra
+
+
+def expected_scr(conf):
+    for line in open(os.path.join(DATA, "expected.scr")):
+        parts = line.split()
+        if parts and parts[0] == conf:
+            return float(parts[1])
+    raise KeyError(conf)
+
+
 def dna_fixture(start_name, ncat):
     order, rows = read_nexus_matrix(os.path.join(DATA, "z.11x2178.nex"))
     trans, score, params, newick = read_start(os.path.join(DATA, start_name))
@@ -100,6 +163,11 @@ def dna_fixture(start_name, ncat):
         "model": {"r": params["r"], "e": params["e"], "a": params.get("a", [None])[0],
                   "p": params.get("p", [0.0])[0], "ncat": ncat},
         "garli_score": score,
+        # the reference's scoring test of this start tree (tests/scoring/<conf>,
+        # tests/data/expected.scr, allowed error from tests/runtests.sh)
+        "scoring_test": {"conf": start_name.replace(".start", ".conf"),
+                         "expected_scr": expected_scr(start_name.replace(".start", ".conf")),
+                         "allowed": 0.01, "sitelike_extra": wtset_sitelike_extra(pd, masks)},
     }
 
 

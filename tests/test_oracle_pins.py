@@ -2,14 +2,18 @@
 
 Pins: GARLI's [!GarliScore] of the start trees in garli/trunk/tests/data
 (n.G4.start, n.G5.start, c.start), recomputed from the parameters GARLI printed
-with them.  Invariants: Population::RunTests (population.cpp:845-966).
+with them; the reference's scoring tests n.G4.conf / n.G5.conf
+(tests/data/expected.scr), reproduced by the restated BetterFinalOptimization
+(branch lengths, alpha, pinv, frequencies, relative rates) on the start tree.
+Invariants: Population::RunTests (population.cpp:845-966).
 """
 import os
 
 import numpy as np
 import pytest
 
-from conftest import fixture_model, load_fixture
+from conftest import fixture_model, fixture_params, load_fixture, scoring_test_score
+from oracle import modelopt as mo
 from oracle import oracle as orc
 
 PINS = ["z11x2178_nG4.json", "z11x2178_nG5.json", "z11x2178_codon.json"]
@@ -124,3 +128,20 @@ def test_oracle_and_engine_eigensystems_match_garli_linalg():
             Pe = m.U @ np.diag(np.exp(m.eval * m.blen_mult * t)) @ m.Uinv
             assert np.abs(Po - Pref).max() < 1e-13
             assert np.abs(Pe - Pref).max() < 1e-13
+
+
+@pytest.mark.parametrize("name", PINS[:2])
+def test_oracle_final_optimization_reproduces_expected_scr(name):
+    """The reference's scoring test (allowed error 0.01 in tests/runtests.sh; the
+    restatement lands within 1e-5, so the bar here is 1e-4)."""
+    fx, pd, c3, dl = load_fixture(name)
+    fp = fixture_params(fx, pd)
+    P = mo.Params(mo.NUC, fp["pi"], fp["rel"], fp["alpha"], fp["ncat"], fp["pinv"], True, fp["max_pinv"])
+    ot = orc.OracleTree(pd, c3, dl, mo.oracle_model(P))
+    opt = mo.ModelOptimizer(ot, P)
+    lnl, passes, evals = opt.final_optimization(0.01, 31)
+    assert passes >= 10 and evals > 100
+    ot.score(0)
+    scr = scoring_test_score(fx, lnl, ot.site_lnl())
+    assert abs(scr - fx["scoring_test"]["expected_scr"]) < 1e-4, (scr, fx["scoring_test"])
+    assert lnl >= fx["garli_score"] - 1e-6
