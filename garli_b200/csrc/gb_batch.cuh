@@ -106,8 +106,7 @@ __device__ __forceinline__ void batch_edge_chunks(const View &v, const EdgeSmem<
         double aL = 0.0, a1 = 0.0, a2 = 0.0;
         const int p = c * kChunk + threadIdx.x;
         if (p < v.npat) {
-            if (p < v.kpad) edge4_site_cg<double, R, GARLI_SCALE>(v, sm, en.pbuf, en.cbuf, en.tip, p, aL, a1, a2);
-            else edge4_site_cg<float, R, GARLI_SCALE>(v, sm, en.pbuf, en.cbuf, en.tip, p, aL, a1, a2);
+            edge4_site_cg<double, R, GARLI_SCALE>(v, sm, en.pbuf, en.cbuf, en.tip, p, aL, a1, a2);  // plain form: FP64
         }
         block_sum3(aL, a1, a2, sums + 3 * c);
         __syncthreads();
@@ -191,8 +190,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch4(View v, BatchArgs A) {
                 }
                 const int t1 = min(ntiles, t0 + tpi);
                 for (int tile = t0; tile < t1; tile++) {
-                    if (tile * PPB < v.kpad) cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);
-                    else cla4_tile_cg<float, R, GARLI_SCALE>(v, op, PL, PR, tile);
+                    cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // plain form: FP64
                 }
             }
             if (!grid_barrier(A.gs, v.status)) return;

@@ -5,9 +5,10 @@
 //   k_level4m (kBLevel, one launch per level): CLA updates with one lane per
 //             (pattern, category), the op's P blocks in padded shared memory,
 //             FP64 fused arithmetic, the pattern's power-of-two
-//             normalisation by a shuffle max, FP32 stores with unbiased
-//             stochastic rounding (exact, no division); every lane prefetches
-//             its inputs two tiles ahead with cp.async.
+//             normalisation by a shuffle max, FP32 stores with an 8-bit
+//             mantissa extension (unbiased stochastic rounding of the
+//             extension byte, exact, no division); every lane prefetches its
+//             inputs two tiles ahead with cp.async.
 //   k_coef4m  (kBCoef, one launch per step): for every candidate's step, the
 //             spectral coefficients of the branch it optimises.  With
 //             P_r(t) = U diag(exp(s_rk t)) U^-1, s_rk = lambda_k rate_r / (1 - pinv),
@@ -75,55 +76,10 @@ struct MixedArgs {
     int trace_cap;
 };
 
-// 2^k as a double, k in [-1022, 1023]
-__device__ __forceinline__ double pow2d(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
-
-// Unbiased stochastic rounding of a non-negative finite double to float: the
-// upper neighbour with probability (x - lo) / ulp, the uniform variate a hash
-// of `key`.  The gap between the float neighbours is a power of two, so the
-// fraction is an exact scaling (no division).
-__device__ __forceinline__ float round_stochastic_exact(double x, unsigned int key) {
-    const float lo = __double2float_rz(x);
-    const float hi = __int_as_float(__float_as_int(lo) + 1);
-    if (!isfinite(hi)) return lo;
-    const double gap = (double)hi - (double)lo;  // exact: a power of two
-    const int ge = (int)((__double_as_longlong(gap) >> 52) & 0x7ff) - 1023;
-    const double frac = (x - (double)lo) * pow2d(-ge);
-    unsigned int h = key * 0x9E3779B1u;
-    h ^= h >> 15;
-    h *= 0x85EBCA77u;
-    h ^= h >> 13;
-    h *= 0xC2B2AE3Du;
-    h ^= h >> 16;
-    const double u = (double)(h >> 8) * (1.0 / 16777216.0);
-    return u < frac ? hi : lo;
-}
-
-// Unbiased stochastic rounding of a slice's four non-negative finite doubles
-// to float, for the DNA CLA stores: value k goes to its upper float neighbour
-// with probability (x - lo) / (hi - lo), its uniform variate the k-th 16-bit
-// field of one 64-bit hash of `key` (the SplitMix64 finalizer).  hi - lo is a
-// power of two and x - lo is exact, so u (hi - lo) < (x - lo) 2^16 is an exact
-// test (no division); the 16-bit variates round up at most 2^-16 ulp too often.
-__device__ __forceinline__ float4 round_stochastic4(const double d[4], unsigned int key) {
-    unsigned long long h = (unsigned long long)key * 0x9E3779B97F4A7C15ULL;
-    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    h = (h ^ (h >> 27)) * 0x94D049BB133111EBULL;
-    h ^= h >> 31;
-    float o[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const float lo = __double2float_rz(d[k]);
-        const float hi = __uint_as_float(__float_as_uint(lo) + 1);
-        const double u = (double)(unsigned int)((h >> (16 * k)) & 0xffffu);
-        o[k] = (isfinite(hi) && u * ((double)hi - (double)lo) < (d[k] - (double)lo) * 65536.0) ? hi : lo;
-    }
-    return make_float4(o[0], o[1], o[2], o[3]);
-}
-
 // Power-of-two normalisation of one pattern-category slice d[4] (the max over
-// the pattern's G lanes) and its store: FP64 segment as is, FP32 segment with
-// stochastic rounding.  All G lanes of the pattern must call this together.
+// the pattern's G lanes) and its store: FP64 segment as is, FP32 segment as
+// FP32 + extension byte (ext_encode4).  All G lanes of the pattern must call
+// this together.
 template <int R>
 __device__ __forceinline__ void cla_finish_m(const View &v, int dest, bool wide, int p, int r, bool act, double d[4],
                                              int m) {
@@ -145,7 +101,11 @@ __device__ __forceinline__ void cla_finish_m(const View &v, int dest, bool wide,
         float *q = cla_ptr<float>(v, dest, p, R * 4) + r * 4;
         // keyed on the slice's offset in the CLA pool: the same rounding in every run
         const unsigned int key = (unsigned int)((reinterpret_cast<const char *>(q) - v.partials) >> 4);
-        reinterpret_cast<float4 *>(q)[0] = round_stochastic4(d, key);
+        float4 hi;
+        unsigned int e;
+        ext_encode4(d, key, hi, e);
+        reinterpret_cast<float4 *>(q)[0] = hi;
+        cla_ext(v, dest, p, R * 4)[r] = e;
     }
     if (r == 0) v.scalers[(long long)dest * v.npat_pad + p] = m - e;
 }
@@ -168,7 +128,7 @@ __device__ __forceinline__ void pvec_tip(const double *P, int code, double out[4
 }
 
 // Child slice of category r at pattern p in FP64: a wide (FP64) buffer or
-// the FP64 segment holds doubles, the FP32 segment floats.
+// the FP64 segment holds doubles, the FP32 segment floats and their extension bytes.
 template <int R>
 __device__ __forceinline__ void slice_load(const View &v, int b, bool wide, int p, int r, double c[4]) {
     if (wide) {
@@ -177,10 +137,7 @@ __device__ __forceinline__ void slice_load(const View &v, int b, bool wide, int 
         ld4d_cg(cla_ptr<double>(v, b, p, R * 4) + r * 4, c);
     } else {
         const float4 a = __ldcg(reinterpret_cast<const float4 *>(cla_ptr<float>(v, b, p, R * 4) + r * 4));
-        c[0] = a.x;
-        c[1] = a.y;
-        c[2] = a.z;
-        c[3] = a.w;
+        ext_decode4(a, __ldcg(cla_ext(v, b, p, R * 4) + r), c);
     }
 }
 
@@ -267,6 +224,7 @@ __device__ __forceinline__ void cp_issue(const View &v, const DevOp &op, int til
                 cp16(smem_u32(dst + 16), src + 2);
             } else {
                 cp16(smem_u32(dst), cla_ptr<float>(v, b, p, R * 4) + r * 4);
+                cp4(smem_u32(dst + 16), cla_ext(v, b, p, R * 4) + r);
             }
         };
         if (op.kind == kTipTip) {
@@ -316,11 +274,8 @@ __device__ __forceinline__ void cla_tiles_cp(const View &v, const DevOp &op, con
                     out[2] = y.x;
                     out[3] = y.y;
                 } else {
-                    const float4 f = *reinterpret_cast<const float4 *>(src);
-                    out[0] = f.x;
-                    out[1] = f.y;
-                    out[2] = f.z;
-                    out[3] = f.w;
+                    ext_decode4(*reinterpret_cast<const float4 *>(src),
+                                *reinterpret_cast<const unsigned int *>(src + 16), out);
                 }
             };
             double a[4], b[4], x[4], y[4];

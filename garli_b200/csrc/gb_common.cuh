@@ -64,6 +64,61 @@ __device__ __forceinline__ float *cla_ptr<float>(const View &v, int b, int p, in
     return reinterpret_cast<float *>(v.partials + (long long)b * v.cla_bytes + (long long)v.kpad * RS * 8) +
            (long long)(p - v.kpad) * RS;
 }
+// 2^k as a double, k in [-1022, 1023]
+__device__ __forceinline__ double pow2d(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// ---- 4-state precision form: FP32 elements with an 8-bit mantissa extension ----
+// An element x >= 0 of the FP32 segment is kept as hi = x rounded toward zero
+// to float plus one extension byte e, x ~ hi + e ulp(hi) / 256 (e stochastically
+// rounded, unbiased): 32 significant bits in 5 bytes, the representation error
+// below ulp(hi) / 256 <= 2^-31 x for normal hi.  The bytes of a (pattern,
+// category) slice form one 32-bit word (byte k = state k); the words follow
+// the FP32 segment in each buffer, R per pattern.
+__device__ __forceinline__ unsigned int *cla_ext(const View &v, int b, int p, int RS) {
+    return reinterpret_cast<unsigned int *>(v.partials + (long long)b * v.cla_bytes + (long long)v.kpad * RS * 8 +
+                                            (long long)(v.npat_pad - v.kpad) * RS * 4) +
+           (long long)(p - v.kpad) * (RS / 4);
+}
+// ulp(hi) / 256 (hi >= 0 finite; subnormal spacing for hi < 2^-126)
+__device__ __forceinline__ double ext_unit(float hi) {
+    const int E = (int)((__float_as_uint(hi) >> 23) & 0xffu);
+    return pow2d(max(E, 1) - 158);
+}
+__device__ __forceinline__ void ext_decode4(const float4 a, unsigned int e, double c[4]) {
+    c[0] = (double)a.x + (double)(e & 0xffu) * ext_unit(a.x);
+    c[1] = (double)a.y + (double)((e >> 8) & 0xffu) * ext_unit(a.y);
+    c[2] = (double)a.z + (double)((e >> 16) & 0xffu) * ext_unit(a.z);
+    c[3] = (double)a.w + (double)(e >> 24) * ext_unit(a.w);
+}
+// Encode four non-negative finite doubles (below 2^127).  x - hi is exact and
+// ulp(hi) / 256 a power of two, so t = (x - hi) 256 / ulp(hi) in [0, 256) is
+// exact; e = floor(t) + [u < frac(t)], u the k-th 16-bit field of a SplitMix64
+// hash of `key` (the same rounding in every run), e = 256 carried into hi.
+__device__ __forceinline__ void ext_encode4(const double d[4], unsigned int key, float4 &hi4, unsigned int &ext) {
+    unsigned long long h = (unsigned long long)key * 0x9E3779B97F4A7C15ULL;
+    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    h = (h ^ (h >> 27)) * 0x94D049BB133111EBULL;
+    h ^= h >> 31;
+    float o[4];
+    ext = 0u;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float lo = __double2float_rz(d[k]);
+        const int E = (int)((__float_as_uint(lo) >> 23) & 0xffu);
+        const double t = (d[k] - (double)lo) * pow2d(158 - max(E, 1));
+        const double fl = floor(t);
+        const double u = (double)(unsigned int)((h >> (16 * k)) & 0xffffu);
+        unsigned int e = (unsigned int)fl + (u < (t - fl) * 65536.0 ? 1u : 0u);
+        if (e == 256u) {
+            lo = __uint_as_float(__float_as_uint(lo) + 1u);
+            e = 0u;
+        }
+        o[k] = lo;
+        ext |= e << (8 * k);
+    }
+    hi4 = make_float4(o[0], o[1], o[2], o[3]);
+}
+
 // A wide buffer b (precision form, batched pass) holds every pattern in FP64
 // and occupies the slots of buffers b and b + 1.
 __device__ __forceinline__ double *cla_ptr_wide(const View &v, int b, int p, int RS) {

@@ -25,8 +25,6 @@ template <typename ST>
 __device__ __forceinline__ void cla_load(const ST *p, double v[4]);
 template <>
 __device__ __forceinline__ void cla_load<double>(const double *p, double v[4]) { ld4d(p, v); }
-template <>
-__device__ __forceinline__ void cla_load<float>(const float *p, double v[4]) { load4<float>(p, v); }
 // Stochastic rounding of a non-negative double to float: the lower or upper
 // float neighbour with probability given by the position between them, the
 // uniform variate being a hash of the value's address.  Unbiased and, unlike
@@ -50,16 +48,20 @@ __device__ __forceinline__ float round_stochastic(double x, unsigned int key) {
     return u < frac ? hi : lo;
 }
 
+// a slice of the edge kernels: FP64, or FP32 with its extension word e
+template <typename ST>
+__device__ __forceinline__ void cla_load_x(const ST *p, const unsigned int *e, double v[4]);
+template <>
+__device__ __forceinline__ void cla_load_x<double>(const double *p, const unsigned int *, double v[4]) { ld4d(p, v); }
+template <>
+__device__ __forceinline__ void cla_load_x<float>(const float *p, const unsigned int *e, double v[4]) {
+    ext_decode4(__ldg(reinterpret_cast<const float4 *>(p)), __ldg(e), v);
+}
+
 template <typename ST>
 __device__ __forceinline__ void cla_store(ST *p, const double v[4]);
 template <>
 __device__ __forceinline__ void cla_store<double>(double *p, const double v[4]) { st4d(p, v); }
-template <>
-__device__ __forceinline__ void cla_store<float>(float *p, const double v[4]) {
-    const unsigned int key = (unsigned int)(reinterpret_cast<unsigned long long>(p) >> 2);
-    reinterpret_cast<float4 *>(p)[0] = make_float4(round_stochastic(v[0], key), round_stochastic(v[1], key + 1),
-                                                   round_stochastic(v[2], key + 2), round_stochastic(v[3], key + 3));
-}
 
 // (a*b + c*d) + (e*f + g*h): the unrolled 4-rate kernels (tree.cpp:7705-7779, :8319-8376)
 __device__ __forceinline__ double dot4_pair(const double *p, const double c[4]) {
@@ -213,11 +215,9 @@ __global__ void __launch_bounds__(kThreads) k_cla4(View v, LevelOps ops) {
         }
     }
     const int ntiles = (v.npat + PPB - 1) / PPB;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // kpad is a multiple of 128, so a tile never straddles the FP64/FP32 boundary
-        if (tile * PPB < v.kpad) cla4_body<double, R, GARLI_SCALE>(v, op, PL, PR, tile);
-        else cla4_body<float, R, GARLI_SCALE>(v, op, PL, PR, tile);
-    }
+    // the plain form keeps every pattern in FP64 (the precision form's CLA
+    // updates are k_cla4m / k_level4m)
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) cla4_body<double, R, GARLI_SCALE>(v, op, PL, PR, tile);
 }
 
 // Block-level sum of three doubles; thread 0 writes the block's partial sums.
@@ -273,13 +273,19 @@ __device__ __forceinline__ void edge4_site(const View &v, const EdgeSmem<R, DERI
     const int m1 = v.scalers[(long long)pbuf * v.npat_pad + p];
     const int m2 = child_tip ? 0 : v.scalers[(long long)cbuf * v.npat_pad + p];
     const ST *PC = cla_ptr<ST>(v, pbuf, p, R * 4);
+    // the FP32 segment's extension words (precision form)
+    const unsigned int *PE = nullptr, *CE = nullptr;
+    if constexpr (sizeof(ST) == 4) {
+        PE = cla_ext(v, pbuf, p, R * 4);
+        if (!child_tip) CE = cla_ext(v, cbuf, p, R * 4);
+    }
     if (!child_tip) {
         const ST *CC = cla_ptr<ST>(v, cbuf, p, R * 4);
 #pragma unroll
         for (int r = 0; r < R; r++) {
             double part[4], c[4];
-            cla_load<ST>(PC + r * 4, part);
-            cla_load<ST>(CC + r * 4, c);
+            cla_load_x<ST>(PC + r * 4, PE + r, part);
+            cla_load_x<ST>(CC + r * 4, CE + r, c);
             const double rp = sm.RP[r];
 #pragma unroll
             for (int i = 0; i < 4; i++) {
@@ -297,7 +303,7 @@ __device__ __forceinline__ void edge4_site(const View &v, const EdgeSmem<R, DERI
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 double part[4];
-                cla_load<ST>(PC + r * 4, part);
+                cla_load_x<ST>(PC + r * 4, PE + r, part);
 #pragma unroll
                 for (int i = 0; i < 4; i++) L[i] = add(L[i], mul(part[i], sm.RP[r]));
             }
@@ -308,7 +314,7 @@ __device__ __forceinline__ void edge4_site(const View &v, const EdgeSmem<R, DERI
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     double part[4];
-                    cla_load<ST>(PC + r * 4, part);
+                    cla_load_x<ST>(PC + r * 4, PE + r, part);
                     const double rp = sm.RP[r];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {

@@ -38,7 +38,7 @@ struct Instance {
     int ntip = 0, nbuf = 0, S = 0, R = 0, npat = 0, npat_pad = 0, neigen = 0, nmat = 0;
     long flags = 0;
     bool mixed = false;
-    size_t elem = 8;     // storage bytes of the FP32/FP64 bulk segment
+    size_t elem = 8;     // storage bytes an element of the bulk segment (FP64 8, FP32 4, FP32 + extension 5)
     int kpad = 0;        // patterns [0, kpad) stored in FP64 (internal order)
     int kpad_cap = 0;    // FP64 segment size the buffers are laid out for
     int nsm = 148;       // multiprocessors of the device
@@ -513,7 +513,7 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     I->nmat = matrixBufferCount;
     I->mixed = (flags & GB_FLAG_MIXED_FP32) != 0;
     I->flags = I->mixed ? GB_FLAG_MIXED_FP32 : GB_FLAG_PLAIN_FP64;
-    I->elem = I->mixed ? 4 : 8;
+    I->elem = I->mixed ? (stateCount == 4 ? 5 : 4) : 8;  // the 4-state FP32 segment carries extension bytes
     I->rank.assign(partialsBufferCount, 0);
     I->wide.assign(partialsBufferCount, 0);
     I->h_rates.assign(categoryCount, 1.0);
@@ -527,8 +527,11 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         I->kpad_cap = I->kpad = I->npat_pad;
     }
     {
+        // FP32 segment of the 4-state precision form: 4 bytes an element plus
+        // one extension byte (cla_ext)
         const long long RS = (long long)I->R * I->S;
-        I->cla_bytes = (long long)I->kpad_cap * RS * 8 + (long long)(I->npat_pad - I->kpad_cap) * RS * 4;
+        const long long f32 = (I->mixed && I->S == 4) ? 5 : 4;
+        I->cla_bytes = (long long)I->kpad_cap * RS * 8 + (long long)(I->npat_pad - I->kpad_cap) * RS * f32;
         I->cla_bytes = (I->cla_bytes + 255) / 256 * 256;
     }
     I->h_tips.assign((size_t)tipCount * patternCount, stateCount == 4 ? 15 : stateCount);
@@ -1181,10 +1184,26 @@ int gb_get_partials(int instance, int bufferIndex, double *out) {
             std::memcpy(out + (size_t)I->perm[q] * RS, wraw.data() + (size_t)q * RS, RS * sizeof(double));
         return GB_SUCCESS;
     }
+    // 4-state precision form: each FP32 element's extension byte (cla_ext)
+    const bool ext = I->mixed && I->S == 4;
+    const unsigned char *e8 =
+        reinterpret_cast<const unsigned char *>(raw.data() + (size_t)I->kpad * RS * 8 + (size_t)(I->npat_pad - I->kpad) * RS * 4);
     for (int q = 0; q < I->npat; q++) {
         double *dst = out + (size_t)I->perm[q] * RS;
-        for (int k = 0; k < RS; k++)
-            dst[k] = q < I->kpad ? d64[(size_t)q * RS + k] : (double)d32[(size_t)(q - I->kpad) * RS + k];
+        for (int k = 0; k < RS; k++) {
+            if (q < I->kpad) {
+                dst[k] = d64[(size_t)q * RS + k];
+                continue;
+            }
+            const float hi = d32[(size_t)(q - I->kpad) * RS + k];
+            dst[k] = hi;
+            if (ext) {
+                uint32_t bits;
+                std::memcpy(&bits, &hi, 4);
+                const int E = std::max((int)((bits >> 23) & 0xffu), 1);
+                dst[k] += (double)e8[(size_t)(q - I->kpad) * RS + k] * std::ldexp(1.0, E - 158);
+            }
+        }
     }
     return GB_SUCCESS;
 }
@@ -1747,9 +1766,10 @@ int gb_get_newton_state(int instance, int matrixIndex, double *out) {
 // ---------------------------------------------------------------------------
 namespace gb {
 
-static void *batch4_func(int R, bool garli) {
+// the plain form's batched pass (the precision form runs k_batch4m)
+static void *batch4_func(int R) {
 #define GB_CASE(r) \
-    case r: return garli ? (void *)k_batch4<r, true> : (void *)k_batch4<r, false>;
+    case r: return (void *)k_batch4<r, true>;
     switch (R) {
         GB_CASE(1) GB_CASE(2) GB_CASE(3) GB_CASE(4) GB_CASE(5) GB_CASE(6) GB_CASE(7) default : GB_CASE(8)
     }
@@ -1822,7 +1842,7 @@ static void *level4m_func(int R) {
 // commands between them in the persistent kernel.
 static int enqueue_batch(Instance *I, const BatchPlan &P, NrParams prm, int rescaleEvery, int tiles, int chunks,
                          bool use_graph) {
-    void *func = I->mixed ? batch4m_func(I->R) : batch4_func(I->R, true);
+    void *func = I->mixed ? batch4m_func(I->R) : batch4_func(I->R);
     int nlev = 0;
     if (I->mixed)
         while (nlev < (int)P.cmds.size() && P.cmds[nlev].type == kBLevel) nlev++;

@@ -109,11 +109,6 @@ template <typename ST>
 __device__ __forceinline__ void cla_load_cg(const ST *p, double v[4]);
 template <>
 __device__ __forceinline__ void cla_load_cg<double>(const double *p, double v[4]) { ld4d_cg(p, v); }
-template <>
-__device__ __forceinline__ void cla_load_cg<float>(const float *p, double v[4]) {
-    const float4 a = __ldcg(reinterpret_cast<const float4 *>(p));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-}
 
 // P, dP, d2P of all R categories at length t into shared memory (the
 // operations and their order are those of pmat_body / Model::CalcDerivatives)
@@ -381,8 +376,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(View v, PassArgs A) {
                         PR[i] = __ldcg(m2 + i);
                     }
                 }
-                if (tile * PPB < v.kpad) cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);
-                else cla4_tile_cg<float, R, GARLI_SCALE>(v, op, PL, PR, tile);
+                cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // plain form: FP64 throughout
             }
             if (!grid_barrier(A.gs, v.status)) return;
             mark(kTrLevelDone);
@@ -409,8 +403,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(View v, PassArgs A) {
                 for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x) {
                     double aL = 0.0, a1 = 0.0, a2 = 0.0;
                     for (int p = vb * kThreads + threadIdx.x; p < v.npat; p += A.nvb * kThreads) {
-                        if (p < v.kpad) edge4_site_cg<double, R, GARLI_SCALE>(v, sm, pbuf, cbuf, tip, p, aL, a1, a2);
-                        else edge4_site_cg<float, R, GARLI_SCALE>(v, sm, pbuf, cbuf, tip, p, aL, a1, a2);
+                        edge4_site_cg<double, R, GARLI_SCALE>(v, sm, pbuf, cbuf, tip, p, aL, a1, a2);
                     }
                     block_sum3(aL, a1, a2, sums + 3 * vb);
                     __syncthreads();

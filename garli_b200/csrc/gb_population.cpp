@@ -530,11 +530,12 @@ int build_plan(Pop &p, int nC, const int *child3s, const double *dlens, const in
 // Algorithmic device-memory bytes of one batched pass of the precision form
 // (see gbp_get_counters).
 double plan_bytes(const Pop &p, const Plan &P, int nC, long long sweeps, double *parts3 = nullptr) {
-    // per pattern: a CLA slice is 4R FP32 values and a 4-byte scale exponent
-    // (FP64 values for the parent tree's wide buffers), a tip one byte; a
-    // step's coefficients are 1 + 3R doubles and a scale exponent; a sweep
-    // reads those and the pattern's count and constant-state word
-    const double cla = 16.0 * p.ncat + 4.0, wide = 32.0 * p.ncat + 4.0;
+    // per pattern: a CLA slice is 4R FP32 values with their extension bytes
+    // and a 4-byte scale exponent (FP64 values for the parent tree's wide
+    // buffers), a tip one byte; a step's coefficients are 1 + 3R doubles and a
+    // scale exponent; a sweep reads those and the pattern's count and
+    // constant-state word
+    const double cla = 20.0 * p.ncat + 4.0, wide = 32.0 * p.ncat + 4.0;
     const double coef = 8.0 * (1 + 3 * p.ncat) + 4.0, sweep = coef + 8.0;
     auto side = [&](int b) {
         if (b < p.ntip) return 1.0;
