@@ -68,55 +68,56 @@ __device__ __forceinline__ float *cla_ptr<float>(const View &v, int b, int p, in
 __device__ __forceinline__ double pow2d(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
 
 // ---- 4-state precision form: FP32 elements with an 8-bit mantissa extension ----
-// An element x >= 0 of the FP32 segment is kept as hi = x rounded toward zero
-// to float plus one extension byte e, x ~ hi + e ulp(hi) / 256 (e stochastically
-// rounded, unbiased): 32 significant bits in 5 bytes, the representation error
-// below ulp(hi) / 256 <= 2^-31 x for normal hi.  The bytes of a (pattern,
-// category) slice form one 32-bit word (byte k = state k); the words follow
-// the FP32 segment in each buffer, R per pattern.
+// An element x >= 0 of the FP32 segment is the double x cut to 32 significant
+// bits: a float word hi (sign, 8-bit exponent, the top 23 mantissa bits) and
+// one extension byte e (the next 8), the 21 bits below rounded stochastically
+// into the 32 (unbiased to 2^-16 of their unit, the variate a hash of the
+// element's place in the pool: the same rounding in every run).  The float
+// word alone is x rounded toward zero to FP32.  Encoding and decoding are
+// integer operations on the IEEE bit fields: the representation error is
+// below 2^-31 x in 5 bytes an element (FP64: 8).  x below 2^-126 (FP32's
+// normal range; the pattern's largest element is in [1, 2)) is stored as 0.
+// The bytes of a (pattern, category) slice form one 32-bit word (byte k =
+// state k); the words follow the FP32 segment in each buffer, R per pattern.
 __device__ __forceinline__ unsigned int *cla_ext(const View &v, int b, int p, int RS) {
     return reinterpret_cast<unsigned int *>(v.partials + (long long)b * v.cla_bytes + (long long)v.kpad * RS * 8 +
                                             (long long)(v.npat_pad - v.kpad) * RS * 4) +
            (long long)(p - v.kpad) * (RS / 4);
 }
-// ulp(hi) / 256 (hi >= 0 finite; subnormal spacing for hi < 2^-126)
-__device__ __forceinline__ double ext_unit(float hi) {
-    const int E = (int)((__float_as_uint(hi) >> 23) & 0xffu);
-    return pow2d(max(E, 1) - 158);
+__device__ __forceinline__ double ext_value(float hi, unsigned int e) {
+    const unsigned int w = __float_as_uint(hi);
+    const unsigned long long E = (w >> 23) & 0xffu;
+    const unsigned long long b = ((E + 896ull) << 52) | ((unsigned long long)(w & 0x7fffffu) << 29) |
+                                 ((unsigned long long)(e & 0xffu) << 21);
+    return E ? __longlong_as_double((long long)b) : 0.0;
 }
 __device__ __forceinline__ void ext_decode4(const float4 a, unsigned int e, double c[4]) {
-    c[0] = (double)a.x + (double)(e & 0xffu) * ext_unit(a.x);
-    c[1] = (double)a.y + (double)((e >> 8) & 0xffu) * ext_unit(a.y);
-    c[2] = (double)a.z + (double)((e >> 16) & 0xffu) * ext_unit(a.z);
-    c[3] = (double)a.w + (double)(e >> 24) * ext_unit(a.w);
+    c[0] = ext_value(a.x, e);
+    c[1] = ext_value(a.y, e >> 8);
+    c[2] = ext_value(a.z, e >> 16);
+    c[3] = ext_value(a.w, e >> 24);
 }
-// Encode four non-negative finite doubles (below 2^127).  x - hi is exact and
-// ulp(hi) / 256 a power of two, so t = (x - hi) 256 / ulp(hi) in [0, 256) is
-// exact; e = floor(t) + [u < frac(t)], u the k-th 16-bit field of a SplitMix64
-// hash of `key` (the same rounding in every run), e = 256 carried into hi.
+// four non-negative finite doubles below 2^128; the k-th 16-bit field of a
+// SplitMix64 hash of `key` is element k's variate
 __device__ __forceinline__ void ext_encode4(const double d[4], unsigned int key, float4 &hi4, unsigned int &ext) {
     unsigned long long h = (unsigned long long)key * 0x9E3779B97F4A7C15ULL;
     h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ULL;
     h = (h ^ (h >> 27)) * 0x94D049BB133111EBULL;
     h ^= h >> 31;
-    float o[4];
+    unsigned int o[4];
     ext = 0u;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        float lo = __double2float_rz(d[k]);
-        const int E = (int)((__float_as_uint(lo) >> 23) & 0xffu);
-        const double t = (d[k] - (double)lo) * pow2d(158 - max(E, 1));
-        const double fl = floor(t);
-        const double u = (double)(unsigned int)((h >> (16 * k)) & 0xffffu);
-        unsigned int e = (unsigned int)fl + (u < (t - fl) * 65536.0 ? 1u : 0u);
-        if (e == 256u) {
-            lo = __uint_as_float(__float_as_uint(lo) + 1u);
-            e = 0u;
-        }
-        o[k] = lo;
-        ext |= e << (8 * k);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(d[k]);
+        const long long E = (long long)(b >> 52) - 896;  // the float exponent field
+        // exponent and 31 mantissa bits, plus one unit with probability (21 low bits) / 2^21
+        unsigned long long c = ((unsigned long long)E << 31) | ((b >> 21) & 0x7fffffffull);
+        const unsigned int u = (unsigned int)((h >> (16 * k)) & 0xffffu) << 5;
+        c += (u < (unsigned int)(b & 0x1fffffull)) ? 1ull : 0ull;
+        o[k] = E > 0 ? (unsigned int)(c >> 8) : 0u;
+        ext |= (E > 0 ? (unsigned int)(c & 0xffull) : 0u) << (8 * k);
     }
-    hi4 = make_float4(o[0], o[1], o[2], o[3]);
+    hi4 = make_float4(__uint_as_float(o[0]), __uint_as_float(o[1]), __uint_as_float(o[2]), __uint_as_float(o[3]));
 }
 
 // A wide buffer b (precision form, batched pass) holds every pattern in FP64

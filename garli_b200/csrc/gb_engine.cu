@@ -1197,11 +1197,15 @@ int gb_get_partials(int instance, int bufferIndex, double *out) {
             }
             const float hi = d32[(size_t)(q - I->kpad) * RS + k];
             dst[k] = hi;
-            if (ext) {
-                uint32_t bits;
-                std::memcpy(&bits, &hi, 4);
-                const int E = std::max((int)((bits >> 23) & 0xffu), 1);
-                dst[k] += (double)e8[(size_t)(q - I->kpad) * RS + k] * std::ldexp(1.0, E - 158);
+            if (ext) {  // the device's ext_value: the float word's fields and the byte as a double
+                uint32_t w;
+                std::memcpy(&w, &hi, 4);
+                const uint64_t E = (w >> 23) & 0xffu;
+                const uint64_t b = ((E + 896u) << 52) | ((uint64_t)(w & 0x7fffffu) << 29) |
+                                   ((uint64_t)e8[(size_t)(q - I->kpad) * RS + k] << 21);
+                double x = 0.0;
+                if (E) std::memcpy(&x, &b, 8);
+                dst[k] = x;
             }
         }
     }
