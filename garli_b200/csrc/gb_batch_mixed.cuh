@@ -110,10 +110,15 @@ __device__ __forceinline__ void cla_finish_m(const View &v, int dest, bool wide,
     if (r == 0) v.scalers[(long long)dest * v.npat_pad + p] = m - e;
 }
 
-// (P c) for the 4 states of one category (P: that category's 4x4 block), FP64 fused
+// (P c) for the 4 states of one category (P: that category's 4x4 block,
+// 16-byte aligned, read as pairs), FP64 fused
 __device__ __forceinline__ void pvec(const double *P, const double c[4], double out[4]) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) out[i] = fma(P[i * 4 + 3], c[3], fma(P[i * 4 + 2], c[2], fma(P[i * 4 + 1], c[1], P[i * 4] * c[0])));
+    for (int i = 0; i < 4; i++) {
+        const double2 lo = *reinterpret_cast<const double2 *>(P + i * 4);
+        const double2 hi = *reinterpret_cast<const double2 *>(P + i * 4 + 2);
+        out[i] = fma(hi.y, c[3], fma(hi.x, c[2], fma(lo.y, c[1], lo.x * c[0])));
+    }
 }
 __device__ __forceinline__ void pvec_tip(const double *P, int code, double out[4]) {
     code &= 15;
@@ -502,9 +507,9 @@ __device__ __forceinline__ void sweep_chunk(const View &v, const MixedArgs &A, i
     }
 }
 
-// P blocks of the current CLA op: [matrix][category][4x4 + 1 pad] (the pad
-// keeps the categories of a warp in different banks)
-constexpr int kPStride = 17;
+// P blocks of the current CLA op: [matrix][category][4x4 + 2 pad] (the pad
+// keeps the categories of a warp in different banks for 16-byte reads)
+constexpr int kPStride = 18;
 
 // A precision-form CLA level as a launch of its own (the per-tree path and the
 // graph-resident pass): the batched kernel's CLA code, blockIdx.y = the op, the
@@ -514,7 +519,7 @@ template <int R>
 __global__ void __launch_bounds__(kThreads, 2) k_cla4m(View v, LevelOps ops) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
-    __shared__ double sP[2][R][kPStride];
+    __shared__ __align__(16) double sP[2][R][kPStride];
     const DevOp op = ops.op[blockIdx.y];
     for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
         const int mi = q / (R * 16), rem = q % (R * 16);
@@ -539,7 +544,7 @@ template <int R>
 __device__ __forceinline__ void level4m_body(const View &v, const DevOp &op, int tpi) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
-    __shared__ double sP[2][R][kPStride];
+    __shared__ __align__(16) double sP[2][R][kPStride];
     extern __shared__ __align__(128) unsigned char dsm[];  // cp_smem_bytes() of prefetch slots
     for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
         const int mi = q / (R * 16), rem = q % (R * 16);
@@ -570,7 +575,7 @@ template <int R>
 __global__ void __launch_bounds__(kThreads, 4) k_coef4m(View v, MixedArgs A, int first_entry, int tpi) {
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
-    __shared__ double sP[2][R][kPStride];
+    __shared__ __align__(16) double sP[2][R][kPStride];
     __shared__ double sUU[32];
     const int e = blockIdx.y;
     const MEntry en = A.entries[first_entry + e];

@@ -260,7 +260,7 @@ __device__ __forceinline__ void block_sum3(double a, double b, double c, double 
 // ---------------------------------------------------------------------------
 template <int R, bool DERIV>
 struct EdgeSmem {
-    double M[3][R * 16];
+    __align__(16) double M[3][R * 16];
     double F[4], RP[R];
 };
 

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass4m(View v, PassArgs A) {
     __shared__ EdgeSmem<R, true> sm;
     __shared__ double red[3][kThreads / 32];
     __shared__ double pscratch[3 * R * 4];
-    __shared__ double sP[2][R][kPStride];
+    __shared__ __align__(16) double sP[2][R][kPStride];
     __shared__ NrState st;
     __shared__ int s_fin;
     const int cr = threadIdx.x % G;
