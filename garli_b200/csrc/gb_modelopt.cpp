@@ -27,11 +27,10 @@
 //   pass p > 0  the proposed value of pass p-1 together with the higher and
 //               lower points of pass p, whose increment is fixed once the
 //               brackets are updated (no widening after pass 0).
-// A speculative score that GARLI would not have computed is never used.  Each
-// candidate model is the model after the previous evaluation with one setter
-// applied; only SetEquilibriumFreq depends on that previous state, through the
-// rounding of the renormalisation, so frequency candidates scored in one batch
-// can differ from GARLI's chained values in the last bits.
+// A speculative score that GARLI would not have computed is never used, and
+// each point's model is built along the chain of setter calls GARLI makes to
+// reach it (SetEquilibriumFreq renormalises the model it is given, so the
+// chain matters in the last bits): the batching changes no result.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -52,7 +51,7 @@ struct Opt {
     std::vector<double> exch;   // fixed amino-acid exchangeabilities
     double lnL = -1.0;          // Tree::lnL (-1: unknown)
     int kmax = 1;               // models one gbt_score_models call can take
-    int depth = 3;              // 0: no batching; 1: known points; >= 2: + speculative widenings
+    int depth = 3;              // 0: no batching; 1: known points; >= 2: + speculative widenings (depth - 1 of them)
     long long evals = 0, scored = 0, calls = 0;
     // evaluations of the last OptimizeBoundedParameter call, in GARLI's order
     double traceInitial = 0.0;
@@ -259,34 +258,47 @@ struct Bounded {
         return m;
     }
 
-    // score, in one batch, the values not already known (each from the current model)
-    int prefetch(const std::vector<double> &vals) {
+    // An evaluation point scored ahead: its value and the point evaluated just
+    // before it on the path the optimiser will take if it reaches it (an index
+    // into the same list; -1: the current model), so that its model is the one
+    // GARLI's chain of setter calls gives.
+    struct Pt {
+        double v;
+        int after;
+    };
+    // score the points in one batch; earlier speculation is dropped
+    int prefetch(const std::vector<Pt> &pts) {
         if (o.depth == 0) return GB_SUCCESS;
-        std::vector<double> todo;
-        for (double v : vals)
-            if (!ahead.count(v) && std::find(todo.begin(), todo.end(), v) == todo.end()) todo.push_back(v);
-        if (todo.empty()) return GB_SUCCESS;
-        std::vector<gb_model_params> ms;
-        for (double v : todo) ms.push_back(with(v));
+        ahead.clear();
+        std::vector<gb_model_params> ms(pts.size());
+        for (size_t k = 0; k < pts.size(); k++) {
+            ms[k] = pts[k].after < 0 ? o.m : ms[pts[k].after];
+            apply(ms[k], param, which, pts[k].v);
+        }
         std::vector<double> lnl;
         int rc = score_batch(o, ms, lnl);
         if (rc) return rc;
-        for (size_t k = 0; k < todo.size(); k++) ahead[todo[k]] = Ahead{ms[k], lnl[k]};
+        for (size_t k = 0; k < pts.size(); k++) ahead.emplace(pts[k].v, Ahead{ms[k], lnl[k]});
         return GB_SUCCESS;
     }
 
-    // SetAndEvaluateParameter (optimization.cpp:244-268)
+    // SetAndEvaluateParameter (optimization.cpp:244-268): a point scored ahead
+    // is used once, else the model is scored now
     int evaluate(double val, double *score) {
         auto it = ahead.find(val);
-        if (it == ahead.end()) {
+        Ahead a;
+        if (it != ahead.end()) {
+            a = it->second;
+            ahead.erase(it);
+        } else {
             std::vector<gb_model_params> ms{with(val)};
             std::vector<double> lnl;
             int rc = score_batch(o, ms, lnl);
             if (rc) return rc;
-            it = ahead.emplace(val, Ahead{ms[0], lnl[0]}).first;
+            a = Ahead{ms[0], lnl[0]};
         }
-        o.m = it->second.m;
-        o.lnL = it->second.lnl;
+        o.m = a.m;
+        o.lnL = a.lnl;
         o.evals++;
         o.traceVal.push_back(val);
         o.traceScore.push_back(o.lnL);
@@ -371,15 +383,21 @@ struct Bounded {
         double upperBracket = highBound, lowerBracket = lowBound;
         {
             // pass 0's points are known now: the bumped value, the first pair and
-            // (speculatively) the pairs of the adaptive widenings
-            std::vector<double> pts;
-            if (bump) pts.push_back(curVal);
+            // (speculatively) the pairs of the adaptive widenings; GARLI's path
+            // through them is bump, higher_0, .., higher_J, lower_J
+            std::vector<Pt> pts;
+            int prev = -1;
+            if (bump) {
+                pts.push_back({curVal, -1});
+                prev = 0;
+            }
             const double incrLimit = std::min(curVal - lowerBracket, upperBracket - curVal);
             const auto inc = pass0_increments(baseIncr, incrLimit, std::max(1, o.depth));
             const int use = o.depth >= 2 ? (int)inc.size() : 1;
             for (int j = 0; j < use; j++) {
-                pts.push_back(curVal + inc[j]);
-                pts.push_back(curVal - inc[j]);
+                pts.push_back({curVal + inc[j], prev});
+                prev = (int)pts.size() - 1;
+                pts.push_back({curVal - inc[j], prev});
             }
             if ((rc = prefetch(pts))) return rc;
         }
@@ -520,7 +538,7 @@ struct Bounded {
             if (o.depth >= 1) {
                 const double lim = std::min(proposed - lowerBracket, upperBracket - proposed);
                 const double nextIncr = baseIncr > lim ? lim / 1.0001 : baseIncr;
-                if ((rc = prefetch({proposed, proposed + nextIncr, proposed - nextIncr}))) return rc;
+                if ((rc = prefetch({{proposed, -1}, {proposed + nextIncr, 0}, {proposed - nextIncr, 1}}))) return rc;
             }
             double proposedScore;
             if ((rc = evaluate(proposed, &proposedScore))) return rc;
@@ -666,6 +684,10 @@ int gbo_create(int tree, const gb_model_params *model, const double *aaExchangea
     o->tree = tree;
     o->inst = inst;
     o->kmax = kmax;
+    // Speculation pays where a rescore costs little next to a call's fixed
+    // latency (small trees); on large ones every model scored is HBM time, so
+    // only the points known for certain are batched.
+    o->depth = (long long)shape[4] * nint <= (1LL << 20) ? 4 : 1;
     if (m.kind == GB_MODEL_AMINO_ACID) o->exch.assign(aaExchangeabilities, aaExchangeabilities + 190);
     if ((rc = install(*o, m))) {
         delete o;

@@ -20,6 +20,8 @@ import numpy as np
 from . import build as _build
 
 GB_SUCCESS = 0
+GB_ERROR_UNINITIALIZED_INSTANCE = -4
+GB_ERROR_OUT_OF_RANGE = -5
 GB_ERROR_RESCALE_RETRY = -9
 GB_FLAG_PLAIN_FP64 = 1 << 0
 GB_FLAG_MIXED_FP32 = 1 << 1

@@ -476,9 +476,11 @@ int gbo_optimize_model(int opt, int mask, double precision, double *out5);
  * OptimizeAllBranches + the parameters in mask until GARLI's exit rule;
  * out[0] = final lnL, out[1] = passes, out[2] = model evaluations */
 int gbo_final_optimization(int opt, double branchOptPrecision, int mask, int maxPasses, double *out3);
-/* 1 (default): evaluation points known in advance are scored in one batch;
- * 0: one model per gbt_score_models call, in GARLI's order */
-int gbo_set_batching(int opt, int on);
+/* depth 0: one model per gbt_score_models call, in GARLI's order; 1: the
+ * evaluation points known in advance are scored together; d >= 2: also the
+ * higher / lower points of the next d - 1 adaptive widenings of pass 0,
+ * speculatively.  Default 4 when patterns x (taxa - 2) <= 2^20, else 1. */
+int gbo_set_batching(int opt, int depth);
 /* the evaluations of the last OptimizeBoundedParameter call in GARLI's order
  * (SetAndEvaluateParameter values and scores, up to capacity) and the score it
  * started from; returns their number */

@@ -162,6 +162,8 @@ class ModelOptimizer:
         self._install()
 
     def _install(self):
+        if self.ot is None:  # replay only: no tree
+            return
         self.ot.set_model(oracle_model(self.p, self.exch))
         self.ot.make_all_dirty()
 

@@ -62,6 +62,20 @@ def fixture_params(fx, pd):
                 max_pinv=nconst / float(np.sum(pd.counts)))
 
 
+def scoring_setup(fx, pd):
+    """Model parameters of a fixture and the parameters its scoring test
+    estimates (tests/scoring/<conf>): n.G4 / n.G5 alpha, pinv, frequencies and
+    six relative rates (mask 15); c.conf six relative rates, omega fixed,
+    empirical codon frequencies (mask 8)."""
+    m = fx["model"]
+    if fx["nstates"] == 4:
+        fp = fixture_params(fx, pd)
+        return dict(kind=0, pi=fp["pi"], rel=fp["rel"], alpha=fp["alpha"], ncat=fp["ncat"], pinv=fp["pinv"],
+                    max_pinv=fp["max_pinv"], omega=1.0, mask=15)
+    return dict(kind=2, pi=np.array(m["e_empirical"], dtype=np.float64), rel=np.array(m["r"], dtype=np.float64),
+                alpha=0.5, ncat=1, pinv=None, max_pinv=0.0, omega=m["o"][0], mask=8)
+
+
 def scoring_test_score(fx, lnl, site_lnl):
     """The number the reference's scoring test compares with expected.scr
     (tests/runtests.sh): -lnL + 1/2 sum (w_c - 1) lnL_c over the weighted

@@ -224,6 +224,10 @@ def codon_fixture(start_name):
         "dlen": dlen.tolist(),
         "model": {"r": params["r"], "e": params["e"], "e_empirical": emp.tolist(), "o": params["o"], "ncat": 1},
         "garli_score": score,
+        # tests/scoring/c.conf: the plain matrix, omega fixed (nonsynonymousfixed),
+        # empirical frequencies, six relative rates estimated
+        "scoring_test": {"conf": "c.conf", "expected_scr": expected_scr("c.conf"), "allowed": 0.01,
+                         "sitelike_extra": []},
     }
 
 

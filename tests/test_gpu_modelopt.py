@@ -10,14 +10,16 @@ and printed parameters.
     oracle's score of that model (1e-9 relative), its evaluations and result
     against oracle/modelopt.py replayed on those scores (exact), speculative
     batching on and off (identical);
-  * gbo_final_optimization (Population::BetterFinalOptimization): the number the
-    reference's scoring test compares with tests/data/expected.scr (allowed
-    error 0.01 in tests/runtests.sh) to 1e-4, and the oracle's final lnL to 1e-6.
+  * gbo_final_optimization (Population::BetterFinalOptimization) on n.G4, n.G5
+    and the codon fixture (GTR+I+G4/G5 with every parameter estimated; codons
+    with six relative rates): the number the reference's scoring test compares
+    with tests/data/expected.scr (allowed error 0.01 in tests/runtests.sh) to
+    1e-4, and the oracle's final lnL to 1e-6.
 """
 import numpy as np
 import pytest
 
-from conftest import fixture_params, load_fixture, scoring_test_score
+from conftest import fixture_params, load_fixture, scoring_setup, scoring_test_score
 from garli_b200 import engine
 from oracle import modelopt as mo
 from oracle import oracle as orc
@@ -173,15 +175,28 @@ def test_optimize_parameter_matches_oracle(name, case):
     _close(opt, tree, inst, ot)
 
 
-@pytest.mark.parametrize("name", FIXTURES)
+def _scoring_sides(name, kmax=8):
+    fx, pd, c3, dl = load_fixture(name)
+    sp = scoring_setup(fx, pd)
+    prm = engine.model_params(sp["kind"], sp["pi"], sp["rel"], sp["alpha"], sp["ncat"], sp["pinv"], sp["max_pinv"],
+                              sp["omega"])
+    inst, tree, opt = engine.model_engine(pd, c3, dl, prm, kmax=kmax)
+    P = mo.Params(sp["kind"], sp["pi"], sp["rel"], sp["alpha"], sp["ncat"], sp["pinv"] or 0.0,
+                  sp["pinv"] is not None, sp["max_pinv"], sp["omega"])
+    ot = orc.OracleTree(pd, c3, dl, mo.oracle_model(P))
+    oopt = mo.ModelOptimizer(ot, P)
+    return fx, pd, sp, (inst, tree, opt), (ot, oopt)
+
+
+@pytest.mark.parametrize("name", FIXTURES + ["z11x2178_codon.json"])
 def test_final_optimization_reproduces_expected_scr(name):
-    fx, pd, (inst, tree, opt), (ot, oopt) = _sides(name)
-    gl, gpasses, gevals = opt.final_optimization(0.01, 31)
+    fx, pd, sp, (inst, tree, opt), (ot, oopt) = _scoring_sides(name)
+    gl, gpasses, gevals = opt.final_optimization(0.01, sp["mask"])
     tree.make_all_dirty()
     assert abs(tree.score(0) - gl) <= 1e-9 * abs(gl)
     scr = scoring_test_score(fx, gl, inst.site_lnl())
     assert abs(scr - fx["scoring_test"]["expected_scr"]) < 1e-4, (scr, fx["scoring_test"])
-    ol, opasses, oevals = oopt.final_optimization(0.01, 31)
+    ol, opasses, oevals = oopt.final_optimization(0.01, sp["mask"])
     assert abs(gl - ol) <= 1e-6, (gl, ol)
     assert gpasses == opasses
     _close(opt, tree, inst, ot)

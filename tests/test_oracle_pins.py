@@ -12,7 +12,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import fixture_model, fixture_params, load_fixture, scoring_test_score
+from conftest import fixture_model, load_fixture, scoring_setup, scoring_test_score
 from oracle import modelopt as mo
 from oracle import oracle as orc
 
@@ -130,16 +130,18 @@ def test_oracle_and_engine_eigensystems_match_garli_linalg():
             assert np.abs(Pe - Pref).max() < 1e-13
 
 
-@pytest.mark.parametrize("name", PINS[:2])
+@pytest.mark.parametrize("name", PINS)
 def test_oracle_final_optimization_reproduces_expected_scr(name):
-    """The reference's scoring test (allowed error 0.01 in tests/runtests.sh; the
-    restatement lands within 1e-5, so the bar here is 1e-4)."""
+    """The reference's scoring tests n.G4, n.G5, c (allowed error 0.01 in
+    tests/runtests.sh; the restatement lands within 1e-5, so the bar here is
+    1e-4)."""
     fx, pd, c3, dl = load_fixture(name)
-    fp = fixture_params(fx, pd)
-    P = mo.Params(mo.NUC, fp["pi"], fp["rel"], fp["alpha"], fp["ncat"], fp["pinv"], True, fp["max_pinv"])
+    sp = scoring_setup(fx, pd)
+    P = mo.Params(sp["kind"], sp["pi"], sp["rel"], sp["alpha"], sp["ncat"], sp["pinv"] or 0.0,
+                  sp["pinv"] is not None, sp["max_pinv"], sp["omega"])
     ot = orc.OracleTree(pd, c3, dl, mo.oracle_model(P))
     opt = mo.ModelOptimizer(ot, P)
-    lnl, passes, evals = opt.final_optimization(0.01, 31)
+    lnl, passes, evals = opt.final_optimization(0.01, sp["mask"])
     assert passes >= 10 and evals > 100
     ot.score(0)
     scr = scoring_test_score(fx, lnl, ot.site_lnl())
