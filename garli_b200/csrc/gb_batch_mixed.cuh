@@ -122,6 +122,13 @@ __device__ __forceinline__ void pvec(const double *P, const double c[4], double 
 }
 __device__ __forceinline__ void pvec_tip(const double *P, int code, double out[4]) {
     code &= 15;
+    if ((code & (code - 1)) == 0 && code) {
+        // one state: a column of P (the sum below with its zero terms dropped)
+        const int b = __ffs(code) - 1;
+#pragma unroll
+        for (int i = 0; i < 4; i++) out[i] = P[i * 4 + b];
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         double s = 0.0;
@@ -198,8 +205,8 @@ __device__ __forceinline__ void cla_tiles_m(const View &v, const DevOp &op, cons
 // without block barriers (a lane reads only what it copied).  Two stages at 4
 // CTAs per SM measured faster than three at 3.  Per lane and
 // stage: child 1's slice (32 B), child 2's slice (32 B), and two 16-byte
-// words holding the pattern's scale exponent or tip code (the aligned
-// 16-byte block that contains it).  Layout [stage][field][lane].
+// words holding the pattern's scale exponents (the aligned 16-byte block that
+// contains it).  Tip codes are not copied.  Layout [stage][field][lane].
 constexpr int kCpStages = 2;
 constexpr int kCpLane = 96;  // bytes per lane and stage
 __host__ __device__ constexpr int cp_smem_bytes() { return kCpStages * kCpLane * kThreads; }
@@ -232,18 +239,15 @@ __device__ __forceinline__ void cp_issue(const View &v, const DevOp &op, int til
                 cp4(smem_u32(dst + 16), cla_ext(v, b, p, R * 4) + r);
             }
         };
-        if (op.kind == kTipTip) {
-            cp16(smem_u32(sl.c), v.tips + (long long)op.c1 * v.npat_pad + (p & ~15));
-            cp16(smem_u32(sl.d), v.tips + (long long)op.c2 * v.npat_pad + (p & ~15));
-        } else {
+        // tip codes are read directly at the arithmetic (one byte, shared by the
+        // pattern's lanes and its neighbours: a copy per lane would repeat it)
+        if (op.kind != kTipTip) {
             // the scale exponents only for the lane of category 0 (the one that stores the sum)
             slice(sl.a, op.c1, op.wide & kWideC1);
             if (r == 0) cp16(smem_u32(sl.c), v.scalers + (long long)op.c1 * v.npat_pad + (p & ~3));
             if (op.kind == kIntInt) {
                 slice(sl.b, op.c2, op.wide & kWideC2);
                 if (r == 0) cp16(smem_u32(sl.d), v.scalers + (long long)op.c2 * v.npat_pad + (p & ~3));
-            } else {
-                cp16(smem_u32(sl.d), v.tips + (long long)op.c2 * v.npat_pad + (p & ~15));
             }
         }
     }
@@ -285,8 +289,8 @@ __device__ __forceinline__ void cla_tiles_cp(const View &v, const DevOp &op, con
             };
             double a[4], b[4], x[4], y[4];
             if (op.kind == kTipTip) {
-                pvec_tip(PL, sl.c[p & 15], x);
-                pvec_tip(PR, sl.d[p & 15], y);
+                pvec_tip(PL, __ldg(v.tips + (long long)op.c1 * v.npat_pad + p), x);
+                pvec_tip(PR, __ldg(v.tips + (long long)op.c2 * v.npat_pad + p), y);
             } else {
                 slice(sl.a, op.wide & kWideC1, a);
                 if (r == 0) m = reinterpret_cast<const int *>(sl.c)[p & 3];
@@ -296,7 +300,7 @@ __device__ __forceinline__ void cla_tiles_cp(const View &v, const DevOp &op, con
                     if (r == 0) m += reinterpret_cast<const int *>(sl.d)[p & 3];
                     pvec(PR, b, y);
                 } else {
-                    pvec_tip(PR, sl.d[p & 15], y);
+                    pvec_tip(PR, __ldg(v.tips + (long long)op.c2 * v.npat_pad + p), y);
                 }
             }
 #pragma unroll
