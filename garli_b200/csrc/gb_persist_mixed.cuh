@@ -9,7 +9,9 @@
 //   * CLA levels use the batched kernel's code (cla_tiles_m): one lane per
 //     (pattern, category), the op's P blocks in shared memory, FP64 fused
 //     arithmetic, both children's loads issued before any arithmetic,
-//     division-free stochastic rounding of the FP32 stores;
+//     compact stores; each block updates the patterns whose edge sums it
+//     takes, so levels and branch ends need no grid barrier -- only the
+//     Newton sums do;
 //   * the edge sweep loads the partial and child slices of all categories
 //     first and evaluates P, dP, d2P with fused FP64 multiply-adds.
 #pragma once
@@ -91,9 +93,6 @@ __device__ __forceinline__ void edge4m_site(const View &v, const EdgeSmem<R, tru
     acc2 = fma(cnt, sd2, acc2);
 }
 
-constexpr int kPassTiles = 2;  // CLA tiles (of 256/G patterns) per level work item: a level of one
-                               // op spreads over every CTA
-
 template <int R>
 __global__ void __launch_bounds__(kThreads, 2) k_pass4m(View v, PassArgs A) {
     constexpr int G = Lanes<R>::G;
@@ -118,27 +117,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass4m(View v, PassArgs A) {
         const PCmd cmd = A.cmds[ci];
         mark(cmd.type == kCmdLevel ? kTrLevel : kTrNewton);
         if (cmd.type == kCmdLevel) {
-            const int items_per_op = (ntiles + kPassTiles - 1) / kPassTiles;
-            const long long nitems = (long long)cmd.b * items_per_op;
-            int cur = -1;
-            DevOp op;
-            for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-                const int j = (int)(item / items_per_op);
-                const int t0 = (int)(item % items_per_op) * kPassTiles;
-                if (j != cur) {  // uniform across the block
-                    cur = j;
-                    op = A.ops[cmd.a + j];
-                    __syncthreads();
-                    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
-                        const int mi = q / (R * 16), rem = q % (R * 16);
-                        sP[mi][rem / 16][rem % 16] =
-                            __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
-                    }
-                    __syncthreads();
+            // Pattern-local: for every op of the level this block updates the
+            // 256-pattern chunks whose edge sums it also takes (chunk c belongs
+            // to virtual block c mod nvb, virtual block vb to block vb mod
+            // grid).  An update reads its children at the same patterns, so
+            // what it needs was written by this block: a block barrier orders
+            // it, and the levels need no grid barrier.
+            const int nchunks = (v.npat + kThreads - 1) / kThreads;
+            for (int j = 0; j < cmd.b; j++) {
+                const DevOp op = A.ops[cmd.a + j];
+                __syncthreads();
+                for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+                    const int mi = q / (R * 16), rem = q % (R * 16);
+                    sP[mi][rem / 16][rem % 16] = __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
                 }
-                cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ntiles, t0 + kPassTiles), crr, cla_ok);
+                __syncthreads();
+                for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x)
+                    for (int c = vb; c < nchunks; c += A.nvb)
+                        cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], c * G, min(ntiles, (c + 1) * G), crr, cla_ok);
             }
-            if (!grid_barrier(A.gs, v.status)) return;
+            __syncthreads();
             mark(kTrLevelDone);
             continue;
         }
@@ -207,14 +205,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass4m(View v, PassArgs A) {
             mark(kTrStep);
             if (s_fin) break;
         }
-        if (blockIdx.x == 0) {
+        // Every block took the same steps from the same sums, so every block
+        // holds the same optimised P: each writes it (identical values) and
+        // reads back its own copy in the levels that follow -- no grid barrier.
+        {
             double *mp = const_cast<double *>(v.mats) + (long long)mat * v.mat_stride;
             for (int i = threadIdx.x; i < R * 16; i += blockDim.x) {
                 mp[i] = sm.M[0][i];
                 mp[R * 16 + i] = sm.M[1][i];
                 mp[2 * R * 16 + i] = sm.M[2][i];
             }
-            if (threadIdx.x == 0) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
                 A.lengths[mat] = st.v;
                 NrSlot &sl = A.slots[mat];
                 sl.st = st;
@@ -224,7 +225,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass4m(View v, PassArgs A) {
                 sl.evals = evals;
             }
         }
-        if (!grid_barrier(A.gs, v.status)) return;
+        __syncthreads();
         mark(kTrNewtonDone);
     }
 }
