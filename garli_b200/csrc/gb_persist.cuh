@@ -360,25 +360,29 @@ __global__ void __launch_bounds__(kThreads) k_pass4(View v, PassArgs A) {
         const PCmd cmd = A.cmds[ci];
         mark(cmd.type == kCmdLevel ? kTrLevel : kTrNewton);
         if (cmd.type == kCmdLevel) {
-            const long long nitems = (long long)cmd.b * ntiles;
-            int cur = -1;
-            double PL[16], PR[16];
-            for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-                const int j = (int)(item / ntiles), tile = (int)(item % ntiles);
+            // Pattern-local: for every op of the level this block updates the
+            // 256-pattern chunks whose edge sums it also takes (chunk c belongs
+            // to virtual block c mod nvb, virtual block vb to block vb mod
+            // grid).  An update reads its children at the same patterns and the
+            // rescale rule is per op and pattern, so what it needs was written
+            // by this block: a block barrier orders it, no grid barrier.
+            const int nchunks = (v.npat + kThreads - 1) / kThreads;
+            for (int j = 0; j < cmd.b; j++) {
                 const DevOp op = A.ops[cmd.a + j];
-                if (j != cur) {
-                    cur = j;
-                    const double *m1 = v.mats + (long long)op.p1 * v.mat_stride + 16 * rr;
-                    const double *m2 = v.mats + (long long)op.p2 * v.mat_stride + 16 * rr;
+                double PL[16], PR[16];
+                const double *m1 = v.mats + (long long)op.p1 * v.mat_stride + 16 * rr;
+                const double *m2 = v.mats + (long long)op.p2 * v.mat_stride + 16 * rr;
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        PL[i] = __ldcg(m1 + i);
-                        PR[i] = __ldcg(m2 + i);
-                    }
+                for (int i = 0; i < 16; i++) {
+                    PL[i] = __ldcg(m1 + i);
+                    PR[i] = __ldcg(m2 + i);
                 }
-                cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // plain form: FP64 throughout
+                for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x)
+                    for (int c = vb; c < nchunks; c += A.nvb)
+                        for (int tile = c * G; tile < min(ntiles, (c + 1) * G); tile++)
+                            cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // plain form: FP64 throughout
+                __syncthreads();
             }
-            if (!grid_barrier(A.gs, v.status)) return;
             mark(kTrLevelDone);
         } else {
             const int pbuf = cmd.a, cbuf = cmd.b, tip = cmd.c, mat = cmd.d;
@@ -444,15 +448,18 @@ __global__ void __launch_bounds__(kThreads) k_pass4(View v, PassArgs A) {
                 mark(kTrStep);
                 if (s_fin) break;
             }
-            if (blockIdx.x == 0) {
-                // the branch's final length and P for the CLA updates that follow
+            // The branch's final length and P for the CLA updates that follow.
+            // Every block took the same steps from the same sums and holds the
+            // same P: each writes it (identical values) and reads back its own
+            // copy in the levels that follow -- no grid barrier.
+            {
                 double *mp = const_cast<double *>(v.mats) + (long long)mat * v.mat_stride;
                 for (int i = threadIdx.x; i < R * 16; i += blockDim.x) {
                     mp[i] = sm.M[0][i];
                     mp[R * 16 + i] = sm.M[1][i];
                     mp[2 * R * 16 + i] = sm.M[2][i];
                 }
-                if (threadIdx.x == 0) {
+                if (blockIdx.x == 0 && threadIdx.x == 0) {
                     A.lengths[mat] = st.v;
                     NrSlot &sl = A.slots[mat];
                     sl.st = st;
@@ -462,7 +469,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(View v, PassArgs A) {
                     sl.evals = evals;
                 }
             }
-            if (!grid_barrier(A.gs, v.status)) return;
+            __syncthreads();
             mark(kTrNewtonDone);
         }
     }
