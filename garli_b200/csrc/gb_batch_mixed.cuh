@@ -383,10 +383,21 @@ __device__ __forceinline__ void coef_store(const View &v, const MixedArgs &A, in
 #pragma unroll
     for (int i = 0; i < 4; i++) w[i] = x[i] * y[i] * v.freqs[i];
     const double rp = act ? v.rate_probs[r] : 0.0;
+    // U and U^-1 (16-byte aligned, row-major) read as pairs
+    double U[16], Ui[16];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const double2 u = reinterpret_cast<const double2 *>(sU)[q];
+        const double2 ui = reinterpret_cast<const double2 *>(sUi)[q];
+        U[2 * q] = u.x;
+        U[2 * q + 1] = u.y;
+        Ui[2 * q] = ui.x;
+        Ui[2 * q + 1] = ui.y;
+    }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        const double a_k = fma(w[3], sU[12 + k], fma(w[2], sU[8 + k], fma(w[1], sU[4 + k], w[0] * sU[k])));
-        const double b_k = fma(sUi[k * 4 + 3], z[3], fma(sUi[k * 4 + 2], z[2], fma(sUi[k * 4 + 1], z[1], sUi[k * 4] * z[0])));
+        const double a_k = fma(w[3], U[12 + k], fma(w[2], U[8 + k], fma(w[1], U[4 + k], w[0] * U[k])));
+        const double b_k = fma(Ui[k * 4 + 3], z[3], fma(Ui[k * 4 + 2], z[2], fma(Ui[k * 4 + 1], z[1], Ui[k * 4] * z[0])));
         c[k] = act ? rp * a_k * b_k : 0.0;
     }
     double c0 = c[0];
@@ -580,7 +591,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_coef4m(View v, MixedArgs A, int
     constexpr int G = Lanes<R>::G;
     constexpr int PPB = kThreads / G;
     __shared__ __align__(16) double sP[2][R][kPStride];
-    __shared__ double sUU[32];
+    __shared__ __align__(16) double sUU[32];
     const int e = blockIdx.y;
     const MEntry en = A.entries[first_entry + e];
     for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
