@@ -360,28 +360,53 @@ __global__ void __launch_bounds__(kThreads) k_pass4(View v, PassArgs A) {
         const PCmd cmd = A.cmds[ci];
         mark(cmd.type == kCmdLevel ? kTrLevel : kTrNewton);
         if (cmd.type == kCmdLevel) {
-            // Pattern-local: for every op of the level this block updates the
-            // 256-pattern chunks whose edge sums it also takes (chunk c belongs
-            // to virtual block c mod nvb, virtual block vb to block vb mod
-            // grid).  An update reads its children at the same patterns and the
-            // rescale rule is per op and pattern, so what it needs was written
-            // by this block: a block barrier orders it, no grid barrier.
+            // Pattern-local (enough 256-pattern chunks for half the blocks):
+            // for every op of the level this block updates the chunks whose
+            // edge sums it also takes (chunk c belongs to virtual block c mod
+            // nvb, virtual block vb to block vb mod grid).  An update reads its
+            // children at the same patterns and the rescale rule is per op and
+            // pattern, so what it needs was written by this block: a block
+            // barrier orders it, no grid barrier.  With fewer chunks the
+            // level's (op, tile) items spread over every block and a grid
+            // barrier ends the level.
             const int nchunks = (v.npat + kThreads - 1) / kThreads;
-            for (int j = 0; j < cmd.b; j++) {
-                const DevOp op = A.ops[cmd.a + j];
-                double PL[16], PR[16];
-                const double *m1 = v.mats + (long long)op.p1 * v.mat_stride + 16 * rr;
-                const double *m2 = v.mats + (long long)op.p2 * v.mat_stride + 16 * rr;
+            if (2 * nchunks >= (int)gridDim.x) {
+                for (int j = 0; j < cmd.b; j++) {
+                    const DevOp op = A.ops[cmd.a + j];
+                    double PL[16], PR[16];
+                    const double *m1 = v.mats + (long long)op.p1 * v.mat_stride + 16 * rr;
+                    const double *m2 = v.mats + (long long)op.p2 * v.mat_stride + 16 * rr;
 #pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    PL[i] = __ldcg(m1 + i);
-                    PR[i] = __ldcg(m2 + i);
+                    for (int i = 0; i < 16; i++) {
+                        PL[i] = __ldcg(m1 + i);
+                        PR[i] = __ldcg(m2 + i);
+                    }
+                    for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x)
+                        for (int c = vb; c < nchunks; c += A.nvb)
+                            for (int tile = c * G; tile < min(ntiles, (c + 1) * G); tile++)
+                                cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // FP64 throughout
+                    __syncthreads();
                 }
-                for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x)
-                    for (int c = vb; c < nchunks; c += A.nvb)
-                        for (int tile = c * G; tile < min(ntiles, (c + 1) * G); tile++)
-                            cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // plain form: FP64 throughout
-                __syncthreads();
+            } else {
+                const long long nitems = (long long)cmd.b * ntiles;
+                int cur = -1;
+                double PL[16], PR[16];
+                for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+                    const int j = (int)(item / ntiles), tile = (int)(item % ntiles);
+                    const DevOp op = A.ops[cmd.a + j];
+                    if (j != cur) {
+                        cur = j;
+                        const double *m1 = v.mats + (long long)op.p1 * v.mat_stride + 16 * rr;
+                        const double *m2 = v.mats + (long long)op.p2 * v.mat_stride + 16 * rr;
+#pragma unroll
+                        for (int i = 0; i < 16; i++) {
+                            PL[i] = __ldcg(m1 + i);
+                            PR[i] = __ldcg(m2 + i);
+                        }
+                    }
+                    cla4_tile_cg<double, R, GARLI_SCALE>(v, op, PL, PR, tile);  // plain form: FP64 throughout
+                }
+                if (!grid_barrier(A.gs, v.status)) return;
             }
             mark(kTrLevelDone);
         } else {

@@ -117,26 +117,54 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass4m(View v, PassArgs A) {
         const PCmd cmd = A.cmds[ci];
         mark(cmd.type == kCmdLevel ? kTrLevel : kTrNewton);
         if (cmd.type == kCmdLevel) {
-            // Pattern-local: for every op of the level this block updates the
-            // 256-pattern chunks whose edge sums it also takes (chunk c belongs
-            // to virtual block c mod nvb, virtual block vb to block vb mod
-            // grid).  An update reads its children at the same patterns, so
-            // what it needs was written by this block: a block barrier orders
-            // it, and the levels need no grid barrier.
+            // Pattern-local (enough 256-pattern chunks for half the blocks):
+            // for every op of the level this block updates the chunks whose
+            // edge sums it also takes (chunk c belongs to virtual block c mod
+            // nvb, virtual block vb to block vb mod grid).  An update reads its
+            // children at the same patterns, so what it needs was written by
+            // this block: a block barrier orders it, no grid barrier.  With
+            // fewer chunks the level's (op, tile pair) items spread over every
+            // block and a grid barrier ends the level.
             const int nchunks = (v.npat + kThreads - 1) / kThreads;
-            for (int j = 0; j < cmd.b; j++) {
-                const DevOp op = A.ops[cmd.a + j];
-                __syncthreads();
-                for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
-                    const int mi = q / (R * 16), rem = q % (R * 16);
-                    sP[mi][rem / 16][rem % 16] = __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
+            if (2 * nchunks >= (int)gridDim.x) {
+                for (int j = 0; j < cmd.b; j++) {
+                    const DevOp op = A.ops[cmd.a + j];
+                    __syncthreads();
+                    for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+                        const int mi = q / (R * 16), rem = q % (R * 16);
+                        sP[mi][rem / 16][rem % 16] =
+                            __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
+                    }
+                    __syncthreads();
+                    for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x)
+                        for (int c = vb; c < nchunks; c += A.nvb)
+                            cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], c * G, min(ntiles, (c + 1) * G), crr,
+                                           cla_ok);
                 }
                 __syncthreads();
-                for (int vb = blockIdx.x; vb < A.nvb; vb += gridDim.x)
-                    for (int c = vb; c < nchunks; c += A.nvb)
-                        cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], c * G, min(ntiles, (c + 1) * G), crr, cla_ok);
+            } else {
+                const int items_per_op = (ntiles + 1) / 2;
+                const long long nitems = (long long)cmd.b * items_per_op;
+                int cur = -1;
+                DevOp op;
+                for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+                    const int j = (int)(item / items_per_op);
+                    const int t0 = (int)(item % items_per_op) * 2;
+                    if (j != cur) {  // uniform across the block
+                        cur = j;
+                        op = A.ops[cmd.a + j];
+                        __syncthreads();
+                        for (int q = threadIdx.x; q < 2 * R * 16; q += blockDim.x) {
+                            const int mi = q / (R * 16), rem = q % (R * 16);
+                            sP[mi][rem / 16][rem % 16] =
+                                __ldcg(v.mats + (long long)(mi ? op.p2 : op.p1) * v.mat_stride + rem);
+                        }
+                        __syncthreads();
+                    }
+                    cla_tiles_m<R>(v, op, sP[0][crr], sP[1][crr], t0, min(ntiles, t0 + 2), crr, cla_ok);
+                }
+                if (!grid_barrier(A.gs, v.status)) return;
             }
-            __syncthreads();
             mark(kTrLevelDone);
             continue;
         }
