@@ -46,6 +46,7 @@ struct View {
     int *status;
     double *block_sums;       // kMaxScoreBlocks x 3
     double *site_lnl;         // npat_pad
+    double *site_d1, *site_d2; // npat_pad each: per-site d lnL / dt, d2 lnL / dt2 of a derivative evaluation
     long long cla_bytes;      // bytes per CLA buffer
     long long mat_stride;     // 3 * R * S * S
     int npat, npat_pad, ntip, kpad, has_pinv, rescale_every;

@@ -368,6 +368,10 @@ __device__ __forceinline__ void edge4_site(const View &v, const EdgeSmem<R, DERI
                 mul(sd1, sd1));
         acc1 = add(acc1, mul(cnt, sd1));
         acc2 = add(acc2, mul(cnt, sd2));
+        if (write_sites) {
+            v.site_d1[p] = sd1;
+            v.site_d2[p] = sd2;
+        }
     }
     if (write_sites) v.site_lnl[p] = u;
 }

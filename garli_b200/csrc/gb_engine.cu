@@ -60,6 +60,8 @@ struct Instance {
     double *d_freqs = nullptr, *d_rates = nullptr, *d_rprobs = nullptr;
     int *d_status = nullptr;
     double *d_block_sums = nullptr, *d_result = nullptr, *d_site_lnl = nullptr;
+    double *d_site_d1 = nullptr, *d_site_d2 = nullptr;  // per-site derivatives of the last derivative evaluation
+    bool site_deriv_valid = false;
     // pinned result staging
     double *h_result = nullptr;
     int *h_status = nullptr;
@@ -189,6 +191,8 @@ static View make_view(Instance *I, int slot = 0) {
     v.status = I->d_status;
     v.block_sums = I->d_block_sums;
     v.site_lnl = I->d_site_lnl;
+    v.site_d1 = I->d_site_d1;
+    v.site_d2 = I->d_site_d2;
     v.cla_bytes = I->cla_bytes;
     v.mat_stride = I->mat_stride();
     v.npat = I->npat;
@@ -576,6 +580,8 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
         {(void **)&I->d_block_sums, (size_t)kMaxScoreBlocks * 3 * sizeof(double)},
         {(void **)&I->d_result, 4 * sizeof(double)},
         {(void **)&I->d_site_lnl, P * sizeof(double)},
+        {(void **)&I->d_site_d1, P * sizeof(double)},
+        {(void **)&I->d_site_d2, P * sizeof(double)},
         {(void **)&I->d_len, (size_t)I->nmat * sizeof(double)},
         {(void **)&I->d_slots, (size_t)I->nmat * sizeof(NrSlot)},
         {(void **)&I->d_gsync, sizeof(GridSync)},
@@ -658,7 +664,7 @@ int gb_finalize_instance(int instance) {
     if (I->graph) cudaGraphDestroy(I->graph);
     void *ptrs[] = {I->d_partials, I->d_scalers, I->d_tips, I->d_counts, I->d_const, I->d_mats,
                     I->d_eigen, I->d_freqs, I->d_rates, I->d_rprobs, I->d_status, I->d_block_sums,
-                    I->d_result, I->d_site_lnl, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
+                    I->d_result, I->d_site_lnl, I->d_site_d1, I->d_site_d2, I->d_len, I->d_slots, I->d_gsync, I->d_sums2,
                     I->d_cmds, I->d_pops, I->d_bcmds, I->d_bops, I->d_bentries, I->d_bslots,
                     I->d_chunk_sums, I->d_active, I->d_mentries, I->d_coef, I->d_etab, I->d_cscale,
                     I->d_tctab, I->d_mslots, I->d_multi, I->d_eq, I->d_epi, I->d_ejobs, I->d_esw};
@@ -1054,6 +1060,7 @@ static int edge_enqueue(Instance *I, const gb_scoring_operation *op, int slot, d
         I->ev_edge.emplace_back(e0, e1);
     }
     I->site_valid = true;
+    I->site_deriv_valid = D;
     return GB_SUCCESS;
 }
 
@@ -1159,6 +1166,24 @@ int gb_get_site_log_likelihoods(int instance, double *out) {
     GB_CUDA(cudaMemcpyAsync(tmp.data(), I->d_site_lnl, I->npat * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
     GB_CUDA(cudaStreamSynchronize(I->stream));
     for (int q = 0; q < I->npat; q++) out[I->perm[q]] = tmp[q];
+    return GB_SUCCESS;
+}
+
+// beagleGetSiteDerivatives (subsetcalculationmanager.cpp:440, OutputBeagleSiteValues)
+int gb_get_site_derivatives(int instance, double *outFirst, double *outSecond) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (!outFirst || !outSecond) return GB_ERROR_OUT_OF_RANGE;
+    if (!I->site_deriv_valid) return GB_ERROR_GENERAL;
+    cudaSetDevice(I->device);
+    std::vector<double> a(I->npat), b(I->npat);
+    GB_CUDA(cudaMemcpyAsync(a.data(), I->d_site_d1, I->npat * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaMemcpyAsync(b.data(), I->d_site_d2, I->npat * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    GB_CUDA(cudaStreamSynchronize(I->stream));
+    for (int q = 0; q < I->npat; q++) {
+        outFirst[I->perm[q]] = a[q];
+        outSecond[I->perm[q]] = b[q];
+    }
     return GB_SUCCESS;
 }
 
@@ -1692,6 +1717,7 @@ int gb_newton_pass(int instance, const gb_nr_branch *branches, int branchCount, 
         out[2] = (double)evals;
     }
     I->site_valid = true;
+    I->site_deriv_valid = false;
     if (*I->h_status & kStatusBarrierTimeout) {
         GB_CUDA(cudaMemsetAsync(I->d_status, 0, sizeof(int), I->stream));
         GB_CUDA(cudaStreamSynchronize(I->stream));

@@ -232,13 +232,20 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
             if (GARLI_SCALE) u = sub(sub(log(siteL), (double)m1), (double)m2);
             else u = sub(log(siteL), (double)(m1 + m2) * 0.69314718055994530941723212145818);
             if (write_sites) v.site_lnl[p] = u;
+            double d1 = 0.0, d2 = 0.0;
+            if (DERIV) {
+                d1 = sD1 / siteL;
+                d2 = sub(sD2 / siteL, mul(d1, d1));
+                if (write_sites) {
+                    v.site_d1[p] = d1;
+                    v.site_d2[p] = d2;
+                }
+            }
             // GARLI drops non-negative site lnLs (tree.cpp:6380, optimization.cpp:3378)
             if (u < 0.0) {
                 const double cnt = (double)v.counts[p];
                 accL = add(accL, mul(u, cnt));
                 if (DERIV) {
-                    const double d1 = sD1 / siteL;
-                    const double d2 = sub(sD2 / siteL, mul(d1, d1));
                     acc1 = add(acc1, mul(cnt, d1));
                     acc2 = add(acc2, mul(cnt, d2));
                 }

@@ -93,6 +93,7 @@ SIGNATURES = {
     "gb_update_partials": (C.c_int, [C.c_int, C.POINTER(ClaOperation), C.c_int, C.c_int]),
     "gb_calculate_edge": (C.c_int, [C.c_int, C.POINTER(ScoringOperation), _D]),
     "gb_get_site_log_likelihoods": (C.c_int, [C.c_int, _D]),
+    "gb_get_site_derivatives": (C.c_int, [C.c_int, _D, _D]),
     "gb_get_partials": (C.c_int, [C.c_int, C.c_int, _D]),
     "gb_get_scale_factors": (C.c_int, [C.c_int, C.c_int, _I]),
     "gb_get_transition_matrix": (C.c_int, [C.c_int, C.c_int, C.c_int, _D]),
@@ -353,6 +354,12 @@ class Instance:
         out = np.zeros(self.npat)
         _chk(lib().gb_get_site_log_likelihoods(self.h, _p(out, C.c_double)), "gb_get_site_log_likelihoods")
         return out
+
+    def site_derivatives(self):
+        """Per-pattern d1, d2 of the last derivative edge evaluation."""
+        a, b = np.zeros(self.npat), np.zeros(self.npat)
+        _chk(lib().gb_get_site_derivatives(self.h, _p(a, C.c_double), _p(b, C.c_double)), "gb_get_site_derivatives")
+        return a, b
 
     def partials(self, buf):
         out = np.zeros((self.npat, self.R, self.S))

@@ -163,6 +163,11 @@ int gb_calculate_edges(int instance, const gb_scoring_operation *ops, const int 
                        double *out);
 /* beagleGetSiteLogLikelihoods of the last gb_calculate_edge (unscaled per pattern) */
 int gb_get_site_log_likelihoods(int instance, double *out);
+/* beagleGetSiteDerivatives (subsetcalculationmanager.cpp:440): per pattern
+ * d lnL_p / dt and d2 lnL_p / dt2 of the last edge evaluation, if it was a
+ * derivative one (GB_ERROR_GENERAL otherwise); the pattern-count-weighted sums
+ * are that evaluation's d1 and d2 */
+int gb_get_site_derivatives(int instance, double *outFirst, double *outSecond);
 /* debug read-back (beagleGetPartials / beagleGetScaleFactors); CLA layout
  * [pattern][category][state], converted to FP64 */
 int gb_get_partials(int instance, int bufferIndex, double *out);

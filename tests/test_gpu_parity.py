@@ -271,3 +271,28 @@ def test_device_newton_pass_rescale_retry():
     tree.make_all_dirty()
     lg, lo = tree.score(0), ot.score(0)
     assert abs(lg - lo) <= 1e-8 * abs(lo)
+
+
+@pytest.mark.parametrize("kind,mixed", [("dna", False), ("dna", True), ("aa", False), ("codon", True)])
+def test_site_derivatives(kind, mixed):
+    """gb_get_site_derivatives (beagleGetSiteDerivatives): the per-pattern d1,
+    d2 of a derivative evaluation, weighted by the pattern counts, sum to the
+    evaluation's d1, d2, and the site lnLs to its lnL (1e-9 relative); a
+    score-only evaluation leaves no site derivatives to read."""
+    w = {"dna": lambda: synth.make_dna(24, 1500, 7, pinv_range=(0.05, 0.3)),
+         "aa": lambda: synth.aa(ntax=12, nsites=400), "codon": lambda: synth.codon(ntax=10, ncodons=200)}[kind]()
+    inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model, mixed=mixed)
+    tree.score(0)
+    with pytest.raises(engine.EngineError):
+        inst.site_derivatives()
+    cnt = np.asarray(w.data.counts, dtype=np.float64)
+    for nd in (1, w.data.ntax + 2, w.child3.shape[0] - 1):
+        lnl, d1, d2 = tree.derivatives(nd)
+        s1, s2 = inst.site_derivatives()
+        u = inst.site_lnl()
+        keep = u < 0.0  # the n-state kernels drop non-negative site lnLs, as GARLI does
+        assert abs(np.sum(cnt[keep] * u[keep]) - lnl) <= 1e-9 * abs(lnl)
+        assert abs(np.sum(cnt[keep] * s1[keep]) - d1) <= 1e-9 * max(1.0, abs(d1)), (nd, d1)
+        assert abs(np.sum(cnt[keep] * s2[keep]) - d2) <= 1e-9 * max(1.0, abs(d2)), (nd, d2)
+    tree.close()
+    inst.close()
