@@ -127,6 +127,11 @@ struct Instance {
     double *d_mslots = nullptr;
     double *d_multi = nullptr;  // results of gb_calculate_edges, 3 per edge
     size_t cap_multi = 0;
+    // CLA launch shapes chosen by timing (autotune_levels): blocks per SM the
+    // per-tree precision 4-state level launch aims at, patterns per block of
+    // the n-state CUDA-core CLA kernel; 0 = the built-in choice
+    int lvl_target = 0, ns_tp = 0;
+    bool tune_pending = true;
     // scratch of gb_set_eigen_from_rate_matrices, kept between calls
     double *d_eq = nullptr, *d_epi = nullptr;
     EigenJob *d_ejobs = nullptr;
@@ -252,11 +257,16 @@ static void launch_edge4(int R, int grid, cudaStream_t st, const View &v, int pb
     }
 }
 
-static int ns_cla_tile(const Instance *I, size_t *smem) {
+static size_t ns_cla_smem(const Instance *I, int tp) {
     const int RS = I->R * I->S, RSS = RS * I->S;
+    return (size_t)(2 * RSS + 3 * tp * RS + tp) * 8;
+}
+// the largest tile (<= 64 patterns) that fits 160 KB, or the tuned one
+static int ns_cla_tile(const Instance *I, size_t *smem) {
     int tp = 64;
-    while (tp > 1 && (size_t)(2 * RSS + 3 * tp * RS + tp) * 8 > 160 * 1024) tp >>= 1;
-    *smem = (size_t)(2 * RSS + 3 * tp * RS + tp) * 8;
+    while (tp > 1 && ns_cla_smem(I, tp) > 160 * 1024) tp >>= 1;
+    if (I->ns_tp > 0 && I->ns_tp <= tp) tp = I->ns_tp;
+    *smem = ns_cla_smem(I, tp);
     return tp;
 }
 // the precision form's FP64 pattern segment beside the tensor-core kernel: a
@@ -378,7 +388,7 @@ static void *level4m_ops_func(int R) {
 static dim3 level4m_grid(const Instance *I, int nops, int *tpi) {
     const int G = I->R <= 1 ? 1 : I->R <= 2 ? 2 : I->R <= 4 ? 4 : 8;
     const int ctiles = (I->npat + kThreads / G - 1) / (kThreads / G);
-    const long long want = 16LL * I->nsm;  // blocks in the launch
+    const long long want = (long long)(I->lvl_target > 0 ? I->lvl_target : 16) * I->nsm;  // blocks in the launch
     const long long t = ((long long)ctiles * nops + want - 1) / want;
     *tpi = (int)std::max(1LL, std::min(32LL, t));
     return dim3((ctiles + *tpi - 1) / *tpi, nops);
@@ -446,6 +456,63 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
         }
     }
     return GB_SUCCESS;
+}
+
+// Launch shapes by timing, on the first op list large enough to time (>= 2
+// levels, >= 2^17 pattern-updates): each candidate runs the whole list twice,
+// the second run timed; the fastest is kept.  Every run computes the same
+// values from the same inputs (each pattern's arithmetic does not depend on
+// the shape), so the list's results are in place afterwards.
+static int autotune_levels(Instance *I, const std::vector<std::vector<DevOp>> &levels, int rescaleEvery) {
+    I->tune_pending = false;
+    std::vector<int> cand;
+    int *knob = nullptr;
+    if (I->S == 4 && I->mixed) {
+        cand = {4, 8, 16, 32};
+        knob = &I->lvl_target;
+    } else if (I->S != 4 && !tc_supported(I)) {
+        int tmax = 64;
+        while (tmax > 1 && ns_cla_smem(I, tmax) > 160 * 1024) tmax >>= 1;
+        for (int tp = 8; tp <= tmax; tp *= 2) cand.push_back(tp);
+        knob = &I->ns_tp;
+    }
+    auto run = [&]() -> int {
+        for (const auto &lv : levels) {
+            int rc = launch_level(I, lv, rescaleEvery);
+            if (rc) return rc;
+        }
+        return GB_SUCCESS;
+    };
+    if (cand.size() < 2) return run();
+    const bool timing = I->timing;
+    I->timing = false;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int pick = cand[0], rc = GB_SUCCESS;
+    for (int c : cand) {
+        *knob = c;
+        if ((rc = run())) break;
+        cudaEventRecord(e0, I->stream);
+        if ((rc = run())) break;
+        cudaEventRecord(e1, I->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = GB_ERROR_GENERAL;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    I->timing = timing;
+    *knob = pick;
+    return rc;
 }
 
 static void resolve_timing(Instance *I) {
@@ -1003,10 +1070,34 @@ int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int
     std::vector<std::vector<DevOp>> levels;
     int rc = prepare_ops(I, ops, count, rescaleEvery, levels);
     if (rc) return rc;
+    if (I->tune_pending && levels.size() >= 2 && (long long)count * I->npat >= (1LL << 17))
+        return autotune_levels(I, levels, rescaleEvery);
     for (auto &lv : levels) {
         rc = launch_level(I, lv, rescaleEvery);
         if (rc) return rc;
     }
+    return GB_SUCCESS;
+}
+
+int gb_set_cla_tuning(int instance, int levelBlocksPerSm, int nstateTilePatterns) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    if (levelBlocksPerSm < -1 || levelBlocksPerSm > 64 || nstateTilePatterns < -1 || nstateTilePatterns > 64)
+        return GB_ERROR_OUT_OF_RANGE;
+    if (levelBlocksPerSm > 0) I->lvl_target = levelBlocksPerSm;
+    if (nstateTilePatterns > 0) I->ns_tp = nstateTilePatterns;
+    I->tune_pending = levelBlocksPerSm == 0 || nstateTilePatterns == 0;
+    I->graph_key = 0;
+    return GB_SUCCESS;
+}
+
+int gb_get_cla_tuning(int instance, int *out3) {
+    Instance *I = get(instance);
+    if (!I) return GB_ERROR_UNINITIALIZED_INSTANCE;
+    size_t smem;
+    out3[0] = I->lvl_target > 0 ? I->lvl_target : 16;
+    out3[1] = ns_cla_tile(I, &smem);
+    out3[2] = I->tune_pending ? 1 : 0;
     return GB_SUCCESS;
 }
 

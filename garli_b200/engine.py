@@ -120,6 +120,8 @@ SIGNATURES = {
     "gb_get_batch_tuning": (C.c_int, [C.c_int, _I]),
     "gb_get_batch_timing": (C.c_int, [C.c_int, _D]),
     "gb_set_tensor_cores": (C.c_int, [C.c_int, C.c_int]),
+    "gb_set_cla_tuning": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "gb_get_cla_tuning": (C.c_int, [C.c_int, _I]),
     "gb_set_buffer_precision": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "gb_set_eigen_from_rate_matrices": (C.c_int, [C.c_int, C.c_int, _I, _D, _D, _D, _I]),
     "gbp_create": (C.c_int, [C.c_int, C.c_int, _I, _D, C.c_int]),
@@ -409,6 +411,14 @@ class Instance:
 
     def set_tensor_cores(self, on: bool):
         _chk(lib().gb_set_tensor_cores(self.h, int(on)), "gb_set_tensor_cores")
+
+    def set_cla_tuning(self, level_blocks_per_sm=-1, nstate_tile=-1):
+        _chk(lib().gb_set_cla_tuning(self.h, int(level_blocks_per_sm), int(nstate_tile)), "gb_set_cla_tuning")
+
+    def cla_tuning(self) -> dict:
+        out = np.zeros(3, dtype=np.int32)
+        _chk(lib().gb_get_cla_tuning(self.h, _p(out, C.c_int)), "gb_get_cla_tuning")
+        return {"level_blocks_per_sm": int(out[0]), "nstate_tile": int(out[1]), "pending": bool(out[2])}
 
     def set_model_slot(self, slot, pi, rates, weights, pinv=0.0, has_pinv=False):
         """Frequencies, category rates / weights and pinv read with eigen index ``slot``."""

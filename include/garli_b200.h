@@ -152,6 +152,15 @@ int gb_set_transition_matrix(int instance, int matrixIndex, const double *P, con
  * a GB_ERROR_RESCALE_RETRY condition is reported by the next call that
  * returns results. */
 int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int rescaleEvery);
+/* CLA launch shapes, chosen by timing on the first op list of >= 2 levels and
+ * >= 2^17 pattern-updates (per-tree precision 4-state: the blocks per SM a level
+ * launch aims at, of 4, 8, 16, 32; n-state CUDA-core kernel: patterns per
+ * block, of 8 .. 64).  Each pattern's arithmetic does not depend on the
+ * shape.  0 re-arms the tuning for the next call, -1 keeps the value, > 0
+ * sets it; a call without a 0 turns the tuning off.  out3 = current level
+ * target, n-state tile, tuning pending. */
+int gb_set_cla_tuning(int instance, int levelBlocksPerSm, int nstateTilePatterns);
+int gb_get_cla_tuning(int instance, int *out3);
 /* beagleCalculateEdgeLogLikelihoods (subsetcalculationmanager.cpp:765-901):
  * returns lnL and, when op->derivatives, d1 and d2 in outLnL[0..2]. */
 int gb_calculate_edge(int instance, const gb_scoring_operation *op, double *out);
