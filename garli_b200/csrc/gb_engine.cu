@@ -512,6 +512,7 @@ static int autotune_levels(Instance *I, const std::vector<std::vector<DevOp>> &l
     cudaEventDestroy(e1);
     I->timing = timing;
     *knob = pick;
+    I->graph_key = 0;  // a captured pass graph holds the old shapes
     return rc;
 }
 
