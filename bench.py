@@ -503,8 +503,8 @@ def cpu_baseline(args, bw):
                               "sample": f"{k1} candidates x 2 repeats, {tt1:.1f} s timed"}}
 
 
-def config0(args, device, orc_time=True):
-    """SURVEY config 0 as a measured object: 32 taxa x 2,000 sites, GTR+G4,
+def small_tree(args, device, orc_time=True):
+    """The small single-tree step as a measured object: 32 taxa x 2,000 sites, GTR+G4,
     full-tree rescore + one all-branch Newton pass per step, plain FP64 and
     precision forms (device-timed); GARLI's CPU path on the same step beside
     them is timed by the caller."""
@@ -523,7 +523,7 @@ def config0(args, device, orc_time=True):
     return out, w
 
 
-def config0_cpu(args, w):
+def small_tree_cpu(args, w):
     """GARLI's CPU path on the config-0 step (score + all-branch Newton pass)."""
     from oracle import oracle as orc
 
@@ -725,7 +725,7 @@ def main():
     launches = mixed["launches"]
     for k in ("pop", "inst"):
         mixed.pop(k).close()
-    c0, w0 = (None, None) if args.no_single else config0(args, device)
+    c0, w0 = (None, None) if args.no_single else small_tree(args, device)
     single = None if args.no_single else single_tree(args, device, rank)
     nstate = None if args.no_single else {"aa_20_states": nstate_forms("aa", device),
                                           "codon_61_states": nstate_forms("codon", device)}
@@ -733,7 +733,7 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, bw)
         if c0 is not None:
-            c0["cpu_oracle"] = config0_cpu(args, w0)
+            c0["cpu_oracle"] = small_tree_cpu(args, w0)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -745,14 +745,14 @@ def main():
             "cla_updates_per_step": cnt["cla_ops"], "tuning": tuning,
             "lnl_evals_per_s": edges / (ms / 1000.0),
             "candidates_per_s": len(conn) * ws * args.steps / (ms / 1000.0),
-            "north_star": north,
+            "speedup_vs_plain": north,
             "gpu_launches": launches,
             "e2e": {"value": e2e_sum, "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                     "ms_per_step": e2e_ms, "generations_timed": args.steps},
             "roofline": roof,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
-            "config0": c0,
+            "small_tree_32x2000": c0,
             "single_tree": single,
             "nstate": nstate,
         }

@@ -1,9 +1,9 @@
-"""Parity with the CPU oracle at the benchmark configurations' full sizes (needs a B200).
+"""Parity with the CPU oracle at the benchmark workloads' full sizes (needs a B200).
 
-  config 1  DNA GTR+I+G4, 128 taxa x 100,000 sites (67,010 patterns)
-  config 2  amino acids, 20 states +G4, 64 taxa x 20,000 sites
-  config 3  codons, GY94 61 states, 32 taxa x 5,000 codons
-  config 4  GA generation: candidates of a 64-taxon tree, GTR+G4, 50,000 sites
+  dna_128x100k   DNA GTR+I+G4, 128 taxa x 100,000 sites (67,010 patterns)
+  aa_64x20k      amino acids, 20 states +G4, 64 taxa x 20,000 sites
+  codon_32x5k    codons, GY94 61 states, 32 taxa x 5,000 codons
+  generation     GA generation: candidates of a 64-taxon tree, GTR+G4, 50,000 sites
 
 For lnL the oracle builds its model with its own Q, discrete-gamma and eigen
 code from the same parameters, so the whole chain (model math included) is
@@ -48,7 +48,7 @@ def _workload(name):
     """Workload and the oracle's scores on it (computed once per module)."""
     if name in _CACHE:
         return _CACHE[name]
-    w = {"config1": synth.dna_large, "config2": synth.aa, "config3": synth.codon}[name]()
+    w = {"dna_128x100k": synth.dna_large, "aa_64x20k": synth.aa, "codon_32x5k": synth.codon}[name]()
     ot = orc.OracleTree(w.data, w.child3, w.dlen, w.model_with(orc))
     lnl = ot.score(0)
     ot.close()
@@ -70,7 +70,7 @@ def _workload(name):
     return _CACHE[name]
 
 
-@pytest.mark.parametrize("name", ["config1", "config2", "config3"])
+@pytest.mark.parametrize("name", ["dna_128x100k", "aa_64x20k", "codon_32x5k"])
 def test_plain_fp64_matches_oracle_at_full_size(name):
     w, lo, derivs, clas = _workload(name)
     inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model)
@@ -88,8 +88,8 @@ def test_plain_fp64_matches_oracle_at_full_size(name):
     inst.close()
 
 
-@pytest.mark.parametrize("name,tc", [("config1", False), ("config2", False), ("config2", True),
-                                     ("config3", False), ("config3", True)])
+@pytest.mark.parametrize("name,tc", [("dna_128x100k", False), ("aa_64x20k", False), ("aa_64x20k", True),
+                                     ("codon_32x5k", False), ("codon_32x5k", True)])
 def test_precision_form_matches_oracle_at_full_size(name, tc):
     w, lo, derivs, _ = _workload(name)
     inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model, mixed=True)

@@ -104,7 +104,7 @@ def test_root_choice_and_rescale_invariance():
     assert abs(tree.score(0) - ref) <= 1e-8 * abs(ref)
 
 
-def test_config0_score_and_newton_pass():
+def test_small_tree_score_and_newton_pass():
     """32 taxa x 2,000 sites GTR+G4: full score plus one all-branch Newton pass."""
     w = synth.dna_small()
     inst, tree, ot = _both(w.data, w.child3, w.dlen, w.model, omodel=w.model_with(orc))
