@@ -29,18 +29,22 @@ __device__ __forceinline__ void tile_load(const View &v, int b, int p0, int RS, 
 
 // dynamic shared memory layout for k_cla_ns:
 //   PL[R*S*S], PR[R*S*S], A[TP*R*S], B[TP*R*S], D[TP*R*S], mx[TP], mlt[TP]
+// P is held transposed, [rate][to][from]: the threads of a warp take
+// consecutive "from" states, so each "to" step reads consecutive words
+// (P's rows are S doubles apart: read by rows, 20 states put 8 threads on a bank).
 template <bool GARLI_SCALE>
 __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S, int R, int TP) {
     extern __shared__ double sm[];
     const DevOp op = ops.op[blockIdx.y];
-    const int RS = R * S, RSS = R * S * S;
+    const int RS = R * S, RSS = R * S * S, SS = S * S;
     double *PL = sm, *PR = PL + RSS, *A = PR + RSS, *B = A + TP * RS, *D = B + TP * RS;
     double *mx = D + TP * RS;
     const double *m1 = v.mats + (long long)op.p1 * v.mat_stride;
     const double *m2 = v.mats + (long long)op.p2 * v.mat_stride;
     for (int i = threadIdx.x; i < RSS; i += blockDim.x) {
-        PL[i] = m1[i];
-        PR[i] = m2[i];
+        const int r = i / SS, from = (i % SS) / S, to = i % S;
+        PL[r * SS + to * S + from] = m1[i];
+        PR[r * SS + to * S + from] = m2[i];
     }
     const int p0 = blockIdx.x * TP;
     const int np = min(TP, v.npat - p0);
@@ -50,28 +54,29 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S
     for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
         const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
         const int p = p0 + pl;
-        const double *pl_row = PL + r * S * S + from * S;
-        const double *pr_row = PR + r * S * S + from * S;
+        // P[from][to] of this rate is pl_col[to * S]
+        const double *pl_col = PL + r * SS + from;
+        const double *pr_col = PR + r * SS + from;
         double val;
         if (op.kind == kIntInt) {
             const double *a = A + pl * RS + r * S, *b = B + pl * RS + r * S;
             double L1 = 0.0, R1 = 0.0;
             for (int to = 0; to < S; to++) {
-                L1 = add(L1, mul(pl_row[to], a[to]));
-                R1 = add(R1, mul(pr_row[to], b[to]));
+                L1 = add(L1, mul(pl_col[to * S], a[to]));
+                R1 = add(R1, mul(pr_col[to * S], b[to]));
             }
             val = mul(L1, R1);
         } else if (op.kind == kIntTip) {
             const double *a = A + pl * RS + r * S;
             double acc = 0.0;
-            for (int to = 0; to < S; to++) acc = add(acc, mul(pl_row[to], a[to]));
+            for (int to = 0; to < S; to++) acc = add(acc, mul(pl_col[to * S], a[to]));
             const int s2 = v.tips[(long long)op.c2 * v.npat_pad + p];
-            val = (s2 < S) ? mul(acc, pr_row[s2]) : acc;
+            val = (s2 < S) ? mul(acc, pr_col[s2 * S]) : acc;
         } else {
             const int l = v.tips[(long long)op.c1 * v.npat_pad + p];
             const int rr = v.tips[(long long)op.c2 * v.npat_pad + p];
-            const double tl = (l < S) ? pl_row[l] : 1.0;
-            const double tr = (rr < S) ? pr_row[rr] : 1.0;
+            const double tl = (l < S) ? pl_col[l * S] : 1.0;
+            const double tr = (rr < S) ? pr_col[rr * S] : 1.0;
             val = mul(tl, tr);
         }
         D[o] = val;
@@ -128,10 +133,14 @@ template <bool GARLI_SCALE, bool DERIV>
 __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf, int mat, int child_tip,
                                                       int write_sites, int S, int R, int TP) {
     extern __shared__ double sm[];
-    const int RS = R * S, RSS = R * S * S;
+    const int RS = R * S, RSS = R * S * S, SS = S * S;
     double *M = sm, *C = M + 3 * RSS, *Pp = C + TP * RS, *T = Pp + TP * RS, *F = T + 3 * TP * RS, *RP = F + S;
     const double *mp = v.mats + (long long)mat * v.mat_stride;
-    for (int i = threadIdx.x; i < (DERIV ? 3 : 1) * RSS; i += blockDim.x) M[i] = mp[i];
+    // P, dP, d2P transposed, [matrix][rate][to][from] (as in k_cla_ns)
+    for (int i = threadIdx.x; i < (DERIV ? 3 : 1) * RSS; i += blockDim.x) {
+        const int k = i / RSS, j = i % RSS, r = j / SS, from = (j % SS) / S, to = j % S;
+        M[k * RSS + r * SS + to * S + from] = mp[i];
+    }
     for (int i = threadIdx.x; i < S; i += blockDim.x) F[i] = v.freqs[i];
     for (int i = threadIdx.x; i < R; i += blockDim.x) RP[i] = v.rate_probs[i];
     double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
@@ -144,24 +153,24 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
         for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
             const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
             const int p = p0 + pl;
-            const double *row = M + r * S * S + from * S;
+            const double *col = M + r * SS + from;  // P[from][to] = col[to * S]
             double l = 0.0, a = 0.0, b = 0.0;
             if (!child_tip) {
                 const double *c = C + pl * RS + r * S;
                 for (int to = 0; to < S; to++) {
-                    l = add(l, mul(row[to], c[to]));
+                    l = add(l, mul(col[to * S], c[to]));
                     if (DERIV) {
-                        a = add(a, mul(row[RSS + to], c[to]));
-                        b = add(b, mul(row[2 * RSS + to], c[to]));
+                        a = add(a, mul(col[RSS + to * S], c[to]));
+                        b = add(b, mul(col[2 * RSS + to * S], c[to]));
                     }
                 }
             } else {
                 const int s = v.tips[(long long)cbuf * v.npat_pad + p];
                 if (s < S) {
-                    l = row[s];
+                    l = col[s * S];
                     if (DERIV) {
-                        a = row[RSS + s];
-                        b = row[2 * RSS + s];
+                        a = col[RSS + s * S];
+                        b = col[2 * RSS + s * S];
                     }
                 } else {
                     l = 1.0;  // total ambiguity: partial*freq only, no derivative terms
