@@ -32,12 +32,16 @@ __device__ __forceinline__ void cla_load<double>(const double *p, double v[4]) {
 // take few distinct values, and a deterministic rounding error of such a value
 // would be repeated in every pattern that shares it and add up coherently in
 // the lnL sum.  Deterministic (same address, same value -> same float).
+// The gap hi - lo is one float ulp, a power of two, so the position
+// (x - lo) / gap is formed exactly as a product with its reciprocal 2^(150-E)
+// (E the float exponent field of lo; 2^149 below the normal range).
 __device__ __forceinline__ float round_stochastic(double x, unsigned int key) {
     const float lo = __double2float_rz(x);
     const float hi = __int_as_float(__float_as_int(lo) + 1);
-    const double gap = (double)hi - (double)lo;
-    if (!(gap > 0.0) || !isfinite(hi)) return lo;
-    const double frac = (x - (double)lo) / gap;
+    if ((__float_as_uint(lo) >> 31) || !isfinite(hi)) return lo;
+    const int E = (int)((__float_as_uint(lo) >> 23) & 0xffu);
+    const double inv_gap = __longlong_as_double((long long)(1023 + (E ? 150 - E : 149)) << 52);
+    const double frac = (x - (double)lo) * inv_gap;
     unsigned int h = key * 0x9E3779B1u;
     h ^= h >> 15;
     h *= 0x85EBCA77u;

@@ -119,7 +119,7 @@ struct Instance {
     cudaGraphExec_t bgraph_exec = nullptr;
     unsigned long long bgraph_key = 0;
     int use_batch_graph = 1;
-    int use_tc = 1;  // precision form, 20 / 61 states: CLA updates on the tensor cores
+    int use_tc = 0;  // precision form, 20 / 61 states: CLA updates on the tensor cores
     unsigned char *d_tctab = nullptr;  // per-op P digit tables of a tensor-core level (k_pdigits)
     // model slots, one per eigen index (model_slot_stride doubles each): the
     // instance-wide setters write every slot, gb_set_model_slot one
@@ -257,24 +257,47 @@ static void launch_edge4(int R, int grid, cudaStream_t st, const View &v, int pb
     }
 }
 
-static size_t ns_cla_smem(const Instance *I, int tp) {
-    const int RS = I->R * I->S, RSS = RS * I->S;
-    return (size_t)(2 * RSS + 3 * tp * RS + tp) * 8;
-}
-// the largest tile (<= 64 patterns) that fits 160 KB, or the tuned one
-static int ns_cla_tile(const Instance *I, size_t *smem) {
+static size_t ns_cla_smem(const Instance *I, int tp) { return ns_cla_smem_bytes(I->S, I->R, tp); }
+// patterns of one warp task of k_cla_ns: tiles are multiples of it
+static int ns_pw(const Instance *I) { return I->S <= 20 ? NsTile<20>::PW : NsTile<61>::PW; }
+// the largest tile (<= 64 patterns, a power of two: it divides the
+// 128-pattern FP64 segment) with at most one warp task per warp that fits 200 KB
+static int ns_tp_max(const Instance *I) {
+    const int pw = ns_pw(I);
     int tp = 64;
-    while (tp > 1 && ns_cla_smem(I, tp) > 160 * 1024) tp >>= 1;
-    if (I->ns_tp > 0 && I->ns_tp <= tp) tp = I->ns_tp;
+    while (tp > pw && (I->R * (tp / pw) > kThreads / 32 || ns_cla_smem(I, tp) > 200 * 1024)) tp >>= 1;
+    return tp;
+}
+// that tile, or the tuned one rounded up to a power of two of at least the warp task
+static int ns_cla_tile(const Instance *I, size_t *smem) {
+    int tp = ns_tp_max(I);
+    if (I->ns_tp > 0) {
+        int t = ns_pw(I);
+        while (t < I->ns_tp) t <<= 1;
+        tp = std::min(tp, t);
+    }
     *smem = ns_cla_smem(I, tp);
     return tp;
 }
 // the precision form's FP64 pattern segment beside the tensor-core kernel: a
-// few hundred patterns, so small tiles (many blocks) rather than deep ones
+// few hundred patterns, so the smallest tile (many blocks) rather than deep ones
 static int ns_seg_tile(const Instance *I, size_t *smem) {
-    const int RS = I->R * I->S, RSS = RS * I->S, tp = 8;
-    *smem = (size_t)(2 * RSS + 3 * tp * RS + tp) * 8;
+    const int tp = ns_pw(I);
+    *smem = ns_cla_smem(I, tp);
     return tp;
+}
+static void *ns_cla_func(int S, bool garli) {
+    if (S <= 20) return garli ? (void *)k_cla_ns<true, 20> : (void *)k_cla_ns<false, 20>;
+    return garli ? (void *)k_cla_ns<true, 61> : (void *)k_cla_ns<false, 61>;
+}
+// blocks per op: at most one resident wave over all ops of the launch, each
+// block walking its op's tiles (P staged once per block)
+static dim3 ns_cla_grid(const Instance *I, void *f, size_t smem, int npat, int tp, int nops) {
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kThreads, smem) != cudaSuccess || occ < 1) occ = 1;
+    const int ntiles = (npat + tp - 1) / tp;
+    const int per_op = std::max(1, occ * I->nsm / std::max(1, nops));
+    return dim3(std::max(1, std::min(ntiles, per_op)), nops);
 }
 static int ns_edge_tile(const Instance *I, size_t *smem) {
     const int RS = I->R * I->S, RSS = RS * I->S;
@@ -326,8 +349,9 @@ static int set_smem_attrs() {
             void *f = tc_func(S, R, &sm);
             if (f) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         }
-    GB_CUDA(cudaFuncSetAttribute(k_cla_ns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_cla_ns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    for (int S : {20, 61})
+        for (bool g : {true, false})
+            GB_CUDA(cudaFuncSetAttribute(ns_cla_func(S, g), cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -424,9 +448,11 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             const int tp = tc ? ns_seg_tile(I, &smem) : ns_cla_tile(I, &smem);
             const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
             if (ns_pat > 0) {
-                dim3 grid((ns_pat + tp - 1) / tp, L.n);
-                if (I->mixed) k_cla_ns<false><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
-                else k_cla_ns<true><<<grid, kThreads, smem, I->stream>>>(v, L, I->S, I->R, tp);
+                void *f = ns_cla_func(I->S, !I->mixed);
+                int R = I->R, plim = ns_pat;
+                void *args[] = {&v, &L, &R, (void *)&tp, &plim};
+                GB_CUDA(cudaLaunchKernel(f, ns_cla_grid(I, f, smem, ns_pat, tp, L.n), dim3(kThreads), args, smem,
+                                         I->stream));
             }
             int first = I->kpad / kTcM, nt = I->npat_pad / kTcM - first;
             if (tc && nt > 0) {
@@ -471,9 +497,7 @@ static int autotune_levels(Instance *I, const std::vector<std::vector<DevOp>> &l
         cand = {4, 8, 16, 32};
         knob = &I->lvl_target;
     } else if (I->S != 4 && !tc_supported(I)) {
-        int tmax = 64;
-        while (tmax > 1 && ns_cla_smem(I, tmax) > 160 * 1024) tmax >>= 1;
-        for (int tp = 8; tp <= tmax; tp *= 2) cand.push_back(tp);
+        for (int tp = ns_pw(I); tp <= ns_tp_max(I); tp *= 2) cand.push_back(tp);
         knob = &I->ns_tp;
     }
     auto run = [&]() -> int {
@@ -584,6 +608,9 @@ int gb_create_instance(int tipCount, int partialsBufferCount, int stateCount, in
     I->neigen = eigenBufferCount;
     I->nmat = matrixBufferCount;
     I->mixed = (flags & GB_FLAG_MIXED_FP32) != 0;
+    // the faster CLA path of the precision form as measured on B200: tensor
+    // cores for 61 states, the CUDA-core FP64 kernel for 20
+    I->use_tc = stateCount == 61 ? 1 : 0;
     I->flags = I->mixed ? GB_FLAG_MIXED_FP32 : GB_FLAG_PLAIN_FP64;
     I->elem = I->mixed ? (stateCount == 4 ? 5 : 4) : 8;  // the 4-state FP32 segment carries extension bytes
     I->rank.assign(partialsBufferCount, 0);
@@ -1559,9 +1586,10 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
                     if (tc) tp = ns_seg_tile(I, &smem);
                     const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
                     if (ns_pat > 0) {
-                        void *args[] = {&v, &L, &S, &R, &tp};
-                        rc = B.add(B.g, &prev, garli ? (void *)k_cla_ns<true> : (void *)k_cla_ns<false>,
-                                   dim3((ns_pat + tp - 1) / tp, L.n), smem, args);
+                        int plim = ns_pat;
+                        void *f = ns_cla_func(S, garli);
+                        void *args[] = {&v, &L, &R, &tp, &plim};
+                        rc = B.add(B.g, &prev, f, ns_cla_grid(I, f, smem, ns_pat, tp, L.n), smem, args);
                     }
                     int first = I->kpad / kTcM;
                     int nt = I->npat_pad / kTcM - first;

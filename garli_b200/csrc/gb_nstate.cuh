@@ -2,14 +2,16 @@
 //
 // CUDA-core FP64 versions that keep GARLI's per-site arithmetic order
 // (sequential sums over "to" states, tree.cpp:7843-7910, :8537-8600,
-// :5597-6460, optimization.cpp:2592-3614).  A block owns a tile of TP
-// patterns; the two P(t) sets of the op and the children's tiles are staged
-// in shared memory, each thread produces (pattern, from-state) outputs, and
-// the tile of results stays in shared memory until the per-pattern rescale
-// decision has been taken.
+// :5597-6460, optimization.cpp:2592-3614).  CLA updates: a block stages the
+// op's two P(t) sets in shared memory once and walks pattern tiles, the next
+// tile's inputs arriving by cp.async while a register tile per lane (several
+// patterns x several from-states) is computed.  Edge evaluations: a block
+// owns a tile of patterns, one (pattern, rate, from) term per thread, summed
+// per pattern in the reference's order.
 #pragma once
 #include "gb_common.cuh"
 #include "gb_dna.cuh"
+#include "gb_stage.cuh"
 
 namespace gb {
 
@@ -27,103 +29,350 @@ __device__ __forceinline__ void tile_load(const View &v, int b, int p0, int RS, 
     }
 }
 
-// dynamic shared memory layout for k_cla_ns:
-//   PL[R*S*S], PR[R*S*S], A[TP*R*S], B[TP*R*S], D[TP*R*S], mx[TP], mlt[TP]
-// P is held transposed, [rate][to][from]: the threads of a warp take
-// consecutive "from" states, so each "to" step reads consecutive words
-// (P's rows are S doubles apart: read by rows, 20 states put 8 threads on a bank).
-template <bool GARLI_SCALE>
-__global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int S, int R, int TP) {
-    extern __shared__ double sm[];
+// Register tile of the n-state CLA kernel: the 32 lanes of a warp are NF
+// "from"-state groups x NQ pattern groups; a lane computes F from-states
+// (fg, fg + NF, ...) of Q patterns (qg, qg + NQ, ...) of one rate category, so
+// each P entry read from shared memory serves Q patterns and each child value
+// serves F from-states.
+template <int S>
+struct NsTile {
+    static constexpr int NF = S <= 20 ? 4 : 8;
+    static constexpr int F = (S + NF - 1) / NF;
+    static constexpr int NQ = 32 / NF;
+    static constexpr int Q = 2;
+    static constexpr int PW = NQ * Q;  // patterns of one warp task; tiles are multiples of it
+};
+
+// Row stride (in doubles) of a pattern in a child tile: >= RS and 2 mod 4,
+// so rows start 16-byte aligned and the 16-byte reads of one "to" pair by the
+// pattern groups of a warp fall in distinct banks.
+__host__ __device__ inline int ns_row_stride(int RS) { return RS + (6 - RS % 4) % 4; }
+
+// dynamic shared memory of k_cla_ns in bytes: P sets, two stages of both
+// children's tiles, per-(rate, pattern) maxima and multipliers, then per
+// stage the children's scalers and tip codes
+__host__ __device__ inline size_t ns_cla_smem_bytes(int S, int R, int TP) {
+    const size_t RS = (size_t)R * S, RSP = (size_t)ns_row_stride(R * S);
+    const size_t dbl = 2 * RS * S + 4 * (size_t)TP * RSP + (size_t)R * TP + TP;
+    return (dbl * 8 + 15) / 16 * 16 + 2 * 2 * (size_t)TP * 4 + 2 * 2 * (size_t)TP;
+}
+
+__device__ __forceinline__ void cp8(uint32_t dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+
+// Asynchronous copy of one tile's inputs into a stage: the children's np
+// patterns x RS values pattern-major in rows of RSP doubles (FP64 tiles in
+// 16-byte pieces when RS is even; an FP32 tile's value as a float in the
+// first half of its slot, widened by the same thread after the wait), their
+// scalers (sc[0..TP) child 1, sc[TP..2TP) child 2) and tip codes (tt[0..TP)
+// child 1, tt[TP..2TP) child 2).
+__device__ __forceinline__ void ns_prefetch(const View &v, const DevOp &op, int p0, int np, int RS, int RSP, int TP,
+                                            double *A, double *B, int *sc, uint8_t *tt) {
+    const bool dbl = p0 < v.kpad;
+    for (int c = 0; c < 2; c++) {
+        const bool has_cla = c == 0 ? op.kind != kTipTip : op.kind == kIntInt;
+        const int buf = c == 0 ? op.c1 : op.c2;
+        if (has_cla) {
+            double *dst = c == 0 ? A : B;
+            if (dbl && RS % 2 == 0) {
+                const int H = RS / 2, n = np * H, dpl = blockDim.x / H, dh = blockDim.x % H;
+                const double *src = cla_ptr<double>(v, buf, p0, RS);
+                int pl = threadIdx.x / H, h = threadIdx.x % H;
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    cp16(smem_u32(dst + pl * RSP + 2 * h), src + 2 * i);
+                    pl += dpl;
+                    h += dh;
+                    if (h >= H) { h -= H; pl++; }
+                }
+            } else {
+                const int n = np * RS, dpl = blockDim.x / RS, drs = blockDim.x % RS;
+                int pl = threadIdx.x / RS, rs = threadIdx.x % RS;
+                if (dbl) {
+                    const double *src = cla_ptr<double>(v, buf, p0, RS);
+                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                        cp8(smem_u32(dst + pl * RSP + rs), src + i);
+                        pl += dpl;
+                        rs += drs;
+                        if (rs >= RS) { rs -= RS; pl++; }
+                    }
+                } else {
+                    const float *src = cla_ptr<float>(v, buf, p0, RS);
+                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                        cp4(smem_u32(dst + pl * RSP + rs), src + i);
+                        pl += dpl;
+                        rs += drs;
+                        if (rs >= RS) { rs -= RS; pl++; }
+                    }
+                }
+            }
+            const int *ssrc = v.scalers + (long long)buf * v.npat_pad + p0;
+            for (int q = threadIdx.x; q < np; q += blockDim.x) cp4(smem_u32(sc + c * TP + q), ssrc + q);
+        } else {
+            // a tip child: its codes for the whole tile (inside the padded pattern range)
+            const uint8_t *tsrc = v.tips + (long long)buf * v.npat_pad + p0;
+            for (int q = threadIdx.x; q < TP / 4; q += blockDim.x) cp4(smem_u32(tt + c * TP + 4 * q), tsrc + 4 * q);
+        }
+    }
+}
+
+// Widen the FP32 values this thread copied by ns_prefetch (after its wait):
+// the same slots, in place.
+__device__ __forceinline__ void ns_widen(const DevOp &op, int np, int RS, int RSP, double *A, double *B) {
+    const int n = np * RS, dpl = blockDim.x / RS, drs = blockDim.x % RS;
+    for (int c = 0; c < (op.kind == kIntInt ? 2 : op.kind == kIntTip ? 1 : 0); c++) {
+        double *dst = c == 0 ? A : B;
+        int pl = threadIdx.x / RS, rs = threadIdx.x % RS;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double *e = dst + pl * RSP + rs;
+            *e = (double)*reinterpret_cast<const float *>(e);
+            pl += dpl;
+            rs += drs;
+            if (rs >= RS) { rs -= RS; pl++; }
+        }
+    }
+}
+
+// acc + p * a: GARLI's separate product and sum (plain form), or one fused
+// multiply-add (precision form: its FP32 storage error, 2^-24, dwarfs the
+// difference)
+template <bool FUSED>
+__device__ __forceinline__ double mac(double acc, double p, double a) {
+    if constexpr (FUSED) return __fma_rn(p, a, acc);
+    else return add(acc, mul(p, a));
+}
+
+// One warp task: per lane the products of Q patterns x F from-states of
+// rate r.  P is [from][to] (this rate's block), a child's row of pattern q
+// starts at X + q * RSP (this rate's offset added).  For even S two "to"
+// steps are read per 16-byte load (P rows and child rows are 16-byte aligned);
+// the sums still run over "to" one term at a time.
+template <int S, bool FUSED>
+__device__ __forceinline__ void ns_task(const DevOp &op, const double *pl_r, const double *pr_r, const double *Ar,
+                                        const double *Br, int RSP, const uint8_t *tt, int TP, const int *pl,
+                                        const int *fr, double (&val)[NsTile<S>::Q][NsTile<S>::F]) {
+    constexpr int F = NsTile<S>::F, Q = NsTile<S>::Q;
+    const bool two = op.kind == kIntInt;
+    if (op.kind != kTipTip) {
+        double aL[Q][F], aR[Q][F];
+#pragma unroll
+        for (int j = 0; j < Q; j++)
+#pragma unroll
+            for (int k = 0; k < F; k++) aL[j][k] = aR[j][k] = 0.0;
+        if constexpr (S % 2 == 0) {
+#pragma unroll 2
+            for (int to = 0; to < S; to += 2) {
+                double2 pL[F], pR[F], a[Q], b[Q];
+#pragma unroll
+                for (int k = 0; k < F; k++) pL[k] = *reinterpret_cast<const double2 *>(pl_r + fr[k] * S + to);
+#pragma unroll
+                for (int j = 0; j < Q; j++) a[j] = *reinterpret_cast<const double2 *>(Ar + pl[j] * RSP + to);
+#pragma unroll
+                for (int j = 0; j < Q; j++)
+#pragma unroll
+                    for (int k = 0; k < F; k++) {
+                        aL[j][k] = mac<FUSED>(aL[j][k], pL[k].x, a[j].x);
+                        aL[j][k] = mac<FUSED>(aL[j][k], pL[k].y, a[j].y);
+                    }
+                if (two) {
+#pragma unroll
+                    for (int k = 0; k < F; k++) pR[k] = *reinterpret_cast<const double2 *>(pr_r + fr[k] * S + to);
+#pragma unroll
+                    for (int j = 0; j < Q; j++) b[j] = *reinterpret_cast<const double2 *>(Br + pl[j] * RSP + to);
+#pragma unroll
+                    for (int j = 0; j < Q; j++)
+#pragma unroll
+                        for (int k = 0; k < F; k++) {
+                            aR[j][k] = mac<FUSED>(aR[j][k], pR[k].x, b[j].x);
+                            aR[j][k] = mac<FUSED>(aR[j][k], pR[k].y, b[j].y);
+                        }
+                }
+            }
+        } else {
+#pragma unroll 2
+            for (int to = 0; to < S; to++) {
+                double pL[F], pR[F], a[Q], b[Q];
+#pragma unroll
+                for (int k = 0; k < F; k++) pL[k] = pl_r[fr[k] * S + to];
+#pragma unroll
+                for (int j = 0; j < Q; j++) a[j] = Ar[pl[j] * RSP + to];
+#pragma unroll
+                for (int j = 0; j < Q; j++)
+#pragma unroll
+                    for (int k = 0; k < F; k++) aL[j][k] = mac<FUSED>(aL[j][k], pL[k], a[j]);
+                if (two) {
+#pragma unroll
+                    for (int k = 0; k < F; k++) pR[k] = pr_r[fr[k] * S + to];
+#pragma unroll
+                    for (int j = 0; j < Q; j++) b[j] = Br[pl[j] * RSP + to];
+#pragma unroll
+                    for (int j = 0; j < Q; j++)
+#pragma unroll
+                        for (int k = 0; k < F; k++) aR[j][k] = mac<FUSED>(aR[j][k], pR[k], b[j]);
+                }
+            }
+        }
+        if (two) {
+#pragma unroll
+            for (int j = 0; j < Q; j++)
+#pragma unroll
+                for (int k = 0; k < F; k++) val[j][k] = mul(aL[j][k], aR[j][k]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < Q; j++) {
+                const int s2 = tt[TP + pl[j]];
+#pragma unroll
+                for (int k = 0; k < F; k++)
+                    val[j][k] = (s2 < S) ? mul(aL[j][k], pr_r[fr[k] * S + s2]) : aL[j][k];
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < Q; j++) {
+            const int l = tt[pl[j]], rr = tt[TP + pl[j]];
+#pragma unroll
+            for (int k = 0; k < F; k++) {
+                const double tl = (l < S) ? pl_r[fr[k] * S + l] : 1.0;
+                const double tr = (rr < S) ? pr_r[fr[k] * S + rr] : 1.0;
+                val[j][k] = mul(tl, tr);
+            }
+        }
+    }
+}
+
+// CLA update for S states (CalcFullCLAInternalInternalNState and the
+// internal-terminal / terminal-terminal forms, tree.cpp:7843-7910, :8537-8600,
+// rescaled as RescaleRateHetNState, tree.cpp:3492-3598).  Every output is
+// GARLI's expression in GARLI's order: per child a sequential sum over "to"
+// of P[from][to] * CLA[to], then the product of the two children; without
+// fused multiply-add in the plain form (GARLI_SCALE), fused in the precision
+// form.  A block keeps the op's two P(t) sets in shared memory
+// and walks pattern tiles of TP (grid-stride over plim patterns), two stages
+// deep: the next tile's children, scalers and tip codes arrive by cp.async
+// while the current one is computed.  A tile is R x TP / PW warp tasks (rate,
+// PW patterns), at most one per warp; a task's products stay in registers
+// until the pattern's multiplier is known, then go to the CLA.
+//   shared: PL[R][S][S], PR (P as in global memory), stage 0 and 1: A[TP][RSP],
+//   B[TP][RSP]; mxr[R][TP], mx[TP]; scalers [stage][child][TP] (int), tip codes
+//   [stage][child][TP] (bytes)
+template <bool GARLI_SCALE, int S>
+__global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int R, int TP, int plim) {
+    using T = NsTile<S>;
+    constexpr int NF = T::NF, F = T::F, NQ = T::NQ, Q = T::Q, SS = S * S;
+    extern __shared__ __align__(16) double sm[];
     const DevOp op = ops.op[blockIdx.y];
-    const int RS = R * S, RSS = R * S * S, SS = S * S;
-    double *PL = sm, *PR = PL + RSS, *A = PR + RSS, *B = A + TP * RS, *D = B + TP * RS;
-    double *mx = D + TP * RS;
+    const int RS = R * S, RSS = R * SS, RSP = ns_row_stride(RS);
+    double *PL = sm, *PR = PL + RSS, *stg = PR + RSS, *mxr = stg + 4 * TP * RSP, *mx = mxr + R * TP;
+    char *tail = reinterpret_cast<char *>(sm) + ((size_t)(2 * RSS + 4 * TP * RSP + R * TP + TP) * 8 + 15) / 16 * 16;
+    int *scs = reinterpret_cast<int *>(tail);                  // [stage][child][TP]
+    uint8_t *tts = reinterpret_cast<uint8_t *>(scs + 4 * TP);  // [stage][child][TP]
+    const int ntiles = (plim + TP - 1) / TP;
+    if ((int)blockIdx.x >= ntiles) return;
+    ns_prefetch(v, op, blockIdx.x * TP, min(TP, plim - (int)blockIdx.x * TP), RS, RSP, TP, stg, stg + TP * RSP, scs,
+                tts);
+    cp_commit();
     const double *m1 = v.mats + (long long)op.p1 * v.mat_stride;
     const double *m2 = v.mats + (long long)op.p2 * v.mat_stride;
     for (int i = threadIdx.x; i < RSS; i += blockDim.x) {
-        const int r = i / SS, from = (i % SS) / S, to = i % S;
-        PL[r * SS + to * S + from] = m1[i];
-        PR[r * SS + to * S + from] = m2[i];
+        PL[i] = m1[i];
+        PR[i] = m2[i];
     }
-    const int p0 = blockIdx.x * TP;
-    const int np = min(TP, v.npat - p0);
-    if (op.kind != kTipTip) tile_load(v, op.c1, p0, RS, np * RS, A);
-    if (op.kind == kIntInt) tile_load(v, op.c2, p0, RS, np * RS, B);
-    __syncthreads();
-    for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
-        const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
-        const int p = p0 + pl;
-        // P[from][to] of this rate is pl_col[to * S]
-        const double *pl_col = PL + r * SS + from;
-        const double *pr_col = PR + r * SS + from;
-        double val;
-        if (op.kind == kIntInt) {
-            const double *a = A + pl * RS + r * S, *b = B + pl * RS + r * S;
-            double L1 = 0.0, R1 = 0.0;
-            for (int to = 0; to < S; to++) {
-                L1 = add(L1, mul(pl_col[to * S], a[to]));
-                R1 = add(R1, mul(pr_col[to * S], b[to]));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int fg = lane % NF, qg = lane / NF;
+    const int tasks = R * (TP / T::PW);  // <= warps of the block (host-chosen TP)
+    const bool worker = warp < tasks;
+    const int r = worker ? warp % R : 0, pb = worker ? (warp / R) * T::PW : 0;
+    int fr[F], pl[Q];
+#pragma unroll
+    for (int k = 0; k < F; k++) fr[k] = min(fg + NF * k, S - 1);  // lanes past S compute a copy, store nothing
+#pragma unroll
+    for (int j = 0; j < Q; j++) pl[j] = pb + qg + NQ * j;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int st = it & 1;
+        const int p0 = tile * TP, np = min(TP, plim - p0);
+        double *A = stg + st * 2 * TP * RSP, *B = A + TP * RSP;
+        const int *sc = scs + st * 2 * TP;
+        const uint8_t *tt = tts + st * 2 * TP;
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) {
+            double *An = stg + (st ^ 1) * 2 * TP * RSP;
+            ns_prefetch(v, op, nxt * TP, min(TP, plim - nxt * TP), RS, RSP, TP, An, An + TP * RSP,
+                        scs + (st ^ 1) * 2 * TP, tts + (st ^ 1) * 2 * TP);
+        }
+        cp_commit();
+        cp_wait<1>();
+        if (p0 >= v.kpad) ns_widen(op, np, RS, RSP, A, B);
+        __syncthreads();  // this tile's stage (and P) in shared memory
+        double val[Q][F];
+        if (worker) {
+            ns_task<S, !GARLI_SCALE>(op, PL + r * SS, PR + r * SS, A + r * S, B + r * S, RSP, tt, TP, pl, fr, val);
+#pragma unroll
+            for (int j = 0; j < Q; j++) {
+                double m = val[j][0];
+#pragma unroll
+                for (int k = 1; k < F; k++)
+                    if (fg + NF * k < S) m = val[j][k] > m ? val[j][k] : m;
+#pragma unroll
+                for (int d = 1; d < NF; d <<= 1) {
+                    const double o = __shfl_xor_sync(0xffffffffu, m, d);
+                    m = o > m ? o : m;
+                }
+                if (fg == 0) mxr[r * TP + pl[j]] = m;
             }
-            val = mul(L1, R1);
-        } else if (op.kind == kIntTip) {
-            const double *a = A + pl * RS + r * S;
-            double acc = 0.0;
-            for (int to = 0; to < S; to++) acc = add(acc, mul(pl_col[to * S], a[to]));
-            const int s2 = v.tips[(long long)op.c2 * v.npat_pad + p];
-            val = (s2 < S) ? mul(acc, pr_col[s2 * S]) : acc;
-        } else {
-            const int l = v.tips[(long long)op.c1 * v.npat_pad + p];
-            const int rr = v.tips[(long long)op.c2 * v.npat_pad + p];
-            const double tl = (l < S) ? pl_col[l * S] : 1.0;
-            const double tr = (rr < S) ? pr_col[rr * S] : 1.0;
-            val = mul(tl, tr);
         }
-        D[o] = val;
-    }
-    __syncthreads();
-    // per-pattern largest entry (RescaleRateHetNState, tree.cpp:3492-3598)
-    for (int pl = threadIdx.x; pl < np; pl += blockDim.x) {
-        double large = D[pl * RS] > D[pl * RS + 1] ? D[pl * RS] : D[pl * RS + 1];
-        for (int s = 2; s < RS; s++) large = D[pl * RS + s] > large ? D[pl * RS + s] : large;
-        const int p = p0 + pl;
-        int m = 0;
-        if (op.kind == kIntInt) m = v.scalers[(long long)op.c1 * v.npat_pad + p] + v.scalers[(long long)op.c2 * v.npat_pad + p];
-        else if (op.kind == kIntTip) m = v.scalers[(long long)op.c1 * v.npat_pad + p];
-        double mult = 1.0;
-        if (GARLI_SCALE) {
-            if (op.rescale && large < c_rescale_below) {
-                if (large < c_reduce_below && (v.rescale_every > 2 || large < c_bail_below))
-                    atomicOr(v.status, kStatusRescaleRetry);
-                int idx = 0;
-                while ((idx + 1) < kRescaleTableLen && c_thresh[idx + 1] > large) idx++;
-                mult = c_mult[idx];
-                m += c_incr[idx];
+        __syncthreads();
+        // per-pattern largest entry over all rates and states (RescaleRateHetNState, tree.cpp:3492-3598)
+        for (int q = threadIdx.x; q < np; q += blockDim.x) {
+            double large = mxr[q];
+            for (int rr = 1; rr < R; rr++) large = mxr[rr * TP + q] > large ? mxr[rr * TP + q] : large;
+            int m = 0;
+            if (op.kind == kIntInt) m = sc[q] + sc[TP + q];
+            else if (op.kind == kIntTip) m = sc[q];
+            double mult = 1.0;
+            if (GARLI_SCALE) {
+                if (op.rescale && large < c_rescale_below) {
+                    if (large < c_reduce_below && (v.rescale_every > 2 || large < c_bail_below))
+                        atomicOr(v.status, kStatusRescaleRetry);
+                    int idx = 0;
+                    while ((idx + 1) < kRescaleTableLen && c_thresh[idx + 1] > large) idx++;
+                    mult = c_mult[idx];
+                    m += c_incr[idx];
+                }
+            } else if (large > 0.0) {
+                const int e = ilogb(large);
+                mult = ldexp(1.0, -e);
+                m -= e;
             }
-        } else if (large > 0.0) {
-            const int e = ilogb(large);
-            mult = ldexp(1.0, -e);
-            m -= e;
+            mx[q] = mult;
+            v.scalers[(long long)op.dest * v.npat_pad + p0 + q] = m;
         }
-        mx[pl] = mult;
-        v.scalers[(long long)op.dest * v.npat_pad + p] = m;
+        __syncthreads();
+        if (worker) {
+#pragma unroll
+            for (int j = 0; j < Q; j++) {
+                if (pl[j] >= np) continue;
+                const double mult = mx[pl[j]];
+                if (p0 < v.kpad) {
+                    double *dst = cla_ptr<double>(v, op.dest, p0 + pl[j], RS) + r * S;
+#pragma unroll
+                    for (int k = 0; k < F; k++)
+                        if (fg + NF * k < S) dst[fg + NF * k] = mult != 1.0 ? mul(val[j][k], mult) : val[j][k];
+                } else {
+                    float *dst = cla_ptr<float>(v, op.dest, p0 + pl[j], RS) + r * S;
+#pragma unroll
+                    for (int k = 0; k < F; k++)
+                        if (fg + NF * k < S) {
+                            // keyed on the value's offset in the CLA pool: the same rounding in every run
+                            const unsigned int key =
+                                (unsigned int)((reinterpret_cast<const char *>(dst + fg + NF * k) - v.partials) >> 2);
+                            dst[fg + NF * k] = round_stochastic(mult != 1.0 ? mul(val[j][k], mult) : val[j][k], key);
+                        }
+                }
+            }
+        }
     }
-    __syncthreads();
-    if (p0 < v.kpad) {
-        double *dst = cla_ptr<double>(v, op.dest, p0, RS);
-        for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
-            const double mult = mx[o / RS];
-            dst[o] = mult != 1.0 ? mul(D[o], mult) : D[o];
-        }
-    } else {
-        float *dst = cla_ptr<float>(v, op.dest, p0, RS);
-        for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
-            const double mult = mx[o / RS];
-            // keyed on the value's offset in the CLA pool: the same rounding in every run
-            const unsigned int key = (unsigned int)((reinterpret_cast<const char *>(dst + o) - v.partials) >> 2);
-            dst[o] = round_stochastic(mult != 1.0 ? mul(D[o], mult) : D[o], key);
-        }
-    }
+    cp_wait<0>();
 }
 
 // Edge evaluation for S states: per-(pattern, rate, from) terms computed in
@@ -136,7 +385,8 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
     const int RS = R * S, RSS = R * S * S, SS = S * S;
     double *M = sm, *C = M + 3 * RSS, *Pp = C + TP * RS, *T = Pp + TP * RS, *F = T + 3 * TP * RS, *RP = F + S;
     const double *mp = v.mats + (long long)mat * v.mat_stride;
-    // P, dP, d2P transposed, [matrix][rate][to][from] (as in k_cla_ns)
+    // P, dP, d2P transposed, [matrix][rate][to][from]: the threads of a warp
+    // take consecutive "from" states, so each "to" step reads consecutive words
     for (int i = threadIdx.x; i < (DERIV ? 3 : 1) * RSS; i += blockDim.x) {
         const int k = i / RSS, j = i % RSS, r = j / SS, from = (j % SS) / S, to = j % S;
         M[k * RSS + r * SS + to * S + from] = mp[i];

@@ -155,7 +155,9 @@ int gb_update_partials(int instance, const gb_cla_operation *ops, int count, int
 /* CLA launch shapes, chosen by timing on the first op list of >= 2 levels and
  * >= 2^17 pattern-updates (per-tree precision 4-state: the blocks per SM a level
  * launch aims at, of 4, 8, 16, 32; n-state CUDA-core kernel: patterns per
- * block, of 8 .. 64).  Each pattern's arithmetic does not depend on the
+ * tile, a power of two from the warp task -- 16 patterns for 20 states, 8
+ * for 61 -- up to 64 and to 8 tasks of one rate category each; a set value is
+ * rounded up to the next such tile and capped).  Each pattern's arithmetic does not depend on the
  * shape.  0 re-arms the tuning for the next call, -1 keeps the value, > 0
  * sets it; a call without a 0 turns the tuning off.  out3 = current level
  * target, n-state tile, tuning pending. */
@@ -245,11 +247,11 @@ int gb_get_pass_trace(int instance, unsigned long long *out, int count);
 int gb_get_newton_state(int instance, int matrixIndex, double *out6);
 
 /* precision form, 20 states (up to 4 categories) and 61 states (one
- * category): 1 (default) = CLA updates of the FP32 segment on the tensor cores
+ * category): 1 (default for 61 states) = CLA updates of the FP32 segment on the tensor cores
  * (tcgen05.mma kind::i8: the CLA as 4 and P(t) as 5 base-256 digits over
  * per-row power-of-two scales, exact 32-bit integer accumulation, each P.CLA
- * product within 2.5e-10 of the CLA row's largest entry); 0 = the CUDA-core
- * FP64-arithmetic kernel.  A pattern whose product maximum falls below 2^-64
+ * product within 2.5e-10 of the CLA row's largest entry); 0 (default for 20
+ * states, where it is the faster) = the CUDA-core FP64-arithmetic kernel.  A pattern whose product maximum falls below 2^-64
  * switches the instance to the CUDA-core kernel (the score that saw it returns
  * GB_ERROR_RESCALE_RETRY, and the tree drivers redo it). */
 int gb_set_tensor_cores(int instance, int on);

@@ -63,8 +63,11 @@ def test_level_shape_choices_agree():
 @pytest.mark.parametrize("mixed", [False, True])
 def test_nstate_tile_choices_agree(mixed):
     w = synth.aa(ntax=48, nsites=12000)
-    ref = _run(w, mixed, (-1, 8), tc=False)
-    assert ref[3]["nstate_tile"] == 8
-    _same(_run(w, mixed, (-1, 32), tc=False), ref)
+    ref = _run(w, mixed, (-1, 16), tc=False)
+    assert ref[3]["nstate_tile"] == 16
+    rounded = _run(w, mixed, (-1, 24), tc=False)  # rounded up to the 16-pattern warp task
+    assert rounded[3]["nstate_tile"] == 32
+    _same(rounded, ref)
+    _same(_run(w, mixed, (-1, 64), tc=False), ref)
     auto = _run(w, mixed, None, tc=False)
     _same(auto, ref)
