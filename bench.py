@@ -75,6 +75,9 @@ def parse():
                     help="profiling: only the batched form (no per-tree comparison, no e2e pass)")
     ap.add_argument("--nstate-only", action="store_true",
                     help="profiling: only the 20- and 61-state rescores (tensor cores, CUDA cores, plain)")
+    ap.add_argument("--nstate-tile", type=int, default=0,
+                    help="profiling: fixed pattern tile of the n-state CUDA-core CLA kernel (no autotuning; "
+                         "a profiler's serialised launches would mislead the tile timing)")
     ap.add_argument("--single-only", action="store_true",
                     help="profiling: only the 128x100k single-tree step (precision and plain forms)")
     ap.add_argument("--cpu-sample-cands", type=int, default=24, help="candidates in the CPU baseline sample")
@@ -145,6 +148,18 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def fp64_nominal_instr_per_s():
+    """Nominal FP64 instruction rate of a B200 (no measured FP64 peak exists
+    for this pool): 148 SMs x 64 FP64 lanes x the maximum SM clock; a fused
+    multiply-add, a product or a sum is one instruction."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f)["sm_max_mhz"])
+    except Exception:
+        mhz = 1965.0
+    return 148 * 64 * mhz * 1e6
 
 
 def profiled_traffic():
@@ -389,7 +404,7 @@ def single_tree(args, device, rank):
     return res
 
 
-def nstate_forms(kind, device, reps=3):
+def nstate_forms(kind, device, reps=3, tile=0):
     """Secondary: full-tree rescore of the 20-state (64 taxa x 20,000 sites, +G4)
     or 61-state (32 taxa x 5,000 codons) alignment in the precision form with the
     tensor-core CLA update, the same form on CUDA cores, and the plain FP64 form;
@@ -406,6 +421,8 @@ def nstate_forms(kind, device, reps=3):
         inst, tree = engine.tree_engine(w.data, w.child3, w.dlen, w.model, device=device, mixed=mixed)
         if mixed:
             inst.set_tensor_cores(tc)
+        if tile > 0:
+            inst.set_cla_tuning(-1, tile)
         stream = torch.cuda.ExternalStream(inst.stream_ptr(), device=f"cuda:{device}")
         tree.make_all_dirty()
         lnl = tree.score(0)
@@ -433,8 +450,13 @@ def nstate_forms(kind, device, reps=3):
         if ref is None:
             ref = lnl
         out[name] = {"site_updates_per_s": upd / (ms / 1000.0), "ms_per_rescore": ms / reps, "lnl": lnl,
-                     "dlnl_vs_plain": lnl - ref, "cla_kernel_gbs": gbs,
+                     "dlnl_vs_plain": lnl - ref, "cla_ms_per_rescore": kt["cla_ms"] / 2, "cla_kernel_gbs": gbs,
                      "cla_hbm_frac": gbs / peaks()[0] if gbs else None}
+        if not tc and kt["cla_ms"] > 0:
+            # the CUDA-core kernel is FP64-bound: its FP64 instruction rate against the nominal one
+            ips = kt["cla_fp64_instr"] / (kt["cla_ms"] / 1000.0)
+            out[name]["cla_fp64_instr_per_s"] = ips
+            out[name]["cla_fp64_frac_of_nominal"] = ips / fp64_nominal_instr_per_s()
         tree.close()
         inst.close()
     return out
@@ -641,7 +663,8 @@ def main():
             pg.destroy_process_group()
         return
     if args.nstate_only:
-        res = {"aa_20_states": nstate_forms("aa", device), "codon_61_states": nstate_forms("codon", device)}
+        res = {"aa_20_states": nstate_forms("aa", device, tile=args.nstate_tile),
+               "codon_61_states": nstate_forms("codon", device, tile=args.nstate_tile)}
         if rank == 0:
             print(json.dumps({"nstate_only": True, "nstate": res}))
         if pg:

@@ -34,21 +34,33 @@ __device__ __forceinline__ void cla_load<double>(const double *p, double v[4]) {
 // the lnL sum.  Deterministic (same address, same value -> same float).
 // The gap hi - lo is one float ulp, a power of two, so the position
 // (x - lo) / gap is formed exactly as a product with its reciprocal 2^(150-E)
-// (E the float exponent field of lo; 2^149 below the normal range).
-__device__ __forceinline__ float round_stochastic(double x, unsigned int key) {
-    const float lo = __double2float_rz(x);
-    const float hi = __int_as_float(__float_as_int(lo) + 1);
-    if ((__float_as_uint(lo) >> 31) || !isfinite(hi)) return lo;
-    const int E = (int)((__float_as_uint(lo) >> 23) & 0xffu);
-    const double inv_gap = __longlong_as_double((long long)(1023 + (E ? 150 - E : 149)) << 52);
-    const double frac = (x - (double)lo) * inv_gap;
+// (E the float exponent field of lo; 2^149 below the normal range).  For x in
+// [2^-126, 2^127) the same decision is taken on the bit fields: lo is x's
+// sign, exponent and top 23 mantissa bits, and (x - lo) / gap is x's low 29
+// mantissa bits over 2^29, so u < (x - lo) / gap iff (h >> 8) * 32 < those bits.
+__device__ __forceinline__ unsigned int sr_hash(unsigned int key) {
     unsigned int h = key * 0x9E3779B1u;
     h ^= h >> 15;
     h *= 0x85EBCA77u;
     h ^= h >> 13;
     h *= 0xC2B2AE3Du;
     h ^= h >> 16;
-    const double u = (double)(h >> 8) * (1.0 / 16777216.0);
+    return h;
+}
+__device__ __forceinline__ float round_stochastic(double x, unsigned int key) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    const unsigned int eb = (unsigned int)(b >> 52);  // sign and exponent field
+    if (eb >= 1023u - 126u && eb <= 1023u + 126u) {
+        const unsigned int lo = ((eb - 896u) << 23) | (unsigned int)((b >> 29) & 0x7fffffu);
+        return __uint_as_float(((sr_hash(key) >> 8) << 5) < (unsigned int)(b & 0x1fffffffu) ? lo + 1u : lo);
+    }
+    const float lo = __double2float_rz(x);
+    const float hi = __int_as_float(__float_as_int(lo) + 1);
+    if ((__float_as_uint(lo) >> 31) || !isfinite(hi)) return lo;
+    const int E = (int)((__float_as_uint(lo) >> 23) & 0xffu);
+    const double inv_gap = __longlong_as_double((long long)(1023 + (E ? 150 - E : 149)) << 52);
+    const double frac = (x - (double)lo) * inv_gap;
+    const double u = (double)(sr_hash(key) >> 8) * (1.0 / 16777216.0);
     return u < frac ? hi : lo;
 }
 

@@ -79,7 +79,8 @@ struct Instance {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
     std::vector<long long> ev_updates;
     std::vector<double> ev_bytes;
-    double cla_ms = 0.0, cla_bytes_timed = 0.0;
+    std::vector<double> ev_fp64;  // FP64 instructions of each timed CLA launch
+    double cla_ms = 0.0, cla_bytes_timed = 0.0, cla_fp64_timed = 0.0;
     long long cla_launches_timed = 0, cla_updates_timed = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_edge;
     double edge_ms = 0.0;
@@ -479,6 +480,22 @@ static int launch_level(Instance *I, const std::vector<DevOp> &ops, int rescaleE
             for (int i = 0; i < L.n; i++)
                 b += L.op[i].kind == kIntInt ? 3 * rsb + 12 : L.op[i].kind == kIntTip ? 2 * rsb + 9 : rsb + 6;
             I->ev_bytes.push_back(b * I->npat);
+            // FP64 instructions per pattern of the n-state CUDA-core kernel: per output
+            // (rate, from) S products and S sums per internal child (one fused
+            // instruction each in the precision form) and one product; 4-state
+            // kernels are not counted
+            double f = 0.0;
+            if (I->S != 4) {
+                const double per = I->mixed ? 1.0 : 2.0, S = I->S, RS = (double)I->R * I->S;
+                for (int i = 0; i < L.n; i++) {
+                    const int nint = L.op[i].kind == kIntInt ? 2 : L.op[i].kind == kIntTip ? 1 : 0;
+                    f += RS * (nint * per * S + 1.0);
+                }
+                const bool tc = tc_supported(I);
+                const int ns_pat = tc ? std::min(I->kpad, I->npat) : I->npat;
+                f *= ns_pat;
+            }
+            I->ev_fp64.push_back(f);
         }
     }
     return GB_SUCCESS;
@@ -550,6 +567,7 @@ static void resolve_timing(Instance *I) {
         I->cla_launches_timed++;
         I->cla_updates_timed += I->ev_updates[i];
         I->cla_bytes_timed += I->ev_bytes[i];
+        I->cla_fp64_timed += I->ev_fp64[i];
         cudaEventDestroy(I->ev[i].first);
         cudaEventDestroy(I->ev[i].second);
     }
@@ -564,6 +582,7 @@ static void resolve_timing(Instance *I) {
     I->ev.clear();
     I->ev_updates.clear();
     I->ev_bytes.clear();
+    I->ev_fp64.clear();
     I->ev_edge.clear();
 }
 
@@ -1446,7 +1465,7 @@ int gb_set_kernel_timing(int instance, int on) {
     cudaSetDevice(I->device);
     resolve_timing(I);
     I->timing = on != 0;
-    I->cla_ms = I->edge_ms = I->cla_bytes_timed = 0.0;
+    I->cla_ms = I->edge_ms = I->cla_bytes_timed = I->cla_fp64_timed = 0.0;
     I->cla_launches_timed = I->cla_updates_timed = I->edge_timed = 0;
     return GB_SUCCESS;
 }
@@ -1464,6 +1483,7 @@ int gb_get_kernel_timing(int instance, double *out) {
     out[3] = I->edge_ms;
     out[4] = (double)I->edge_timed;
     out[5] = I->cla_bytes_timed;
+    out[6] = I->cla_fp64_timed;
     return GB_SUCCESS;
 }
 

@@ -63,8 +63,10 @@ __device__ __forceinline__ void cp8(uint32_t dst, const void *src) {
 
 // Asynchronous copy of one tile's inputs into a stage: the children's np
 // patterns x RS values pattern-major in rows of RSP doubles (FP64 tiles in
-// 16-byte pieces when RS is even; an FP32 tile's value as a float in the
-// first half of its slot, widened by the same thread after the wait), their
+// 16-byte pieces when RS is even; FP32 tiles, to be widened after the wait,
+// as 16-byte pieces of floats in the tail of each row's slot when RS is a
+// multiple of 4, else each value as a float in the first half of its slot),
+// their
 // scalers (sc[0..TP) child 1, sc[TP..2TP) child 2) and tip codes (tt[0..TP)
 // child 1, tt[TP..2TP) child 2).
 __device__ __forceinline__ void ns_prefetch(const View &v, const DevOp &op, int p0, int np, int RS, int RSP, int TP,
@@ -84,6 +86,18 @@ __device__ __forceinline__ void ns_prefetch(const View &v, const DevOp &op, int 
                     pl += dpl;
                     h += dh;
                     if (h >= H) { h -= H; pl++; }
+                }
+            } else if (!dbl && RS % 4 == 0) {
+                // FP32 rows in 16-byte pieces into the tail of each row's slot (ns_widen_rows)
+                const int Q4 = RS / 4, n = np * Q4, dpl = blockDim.x / Q4, dq = blockDim.x % Q4;
+                const float *src = cla_ptr<float>(v, buf, p0, RS);
+                const int tail = (RSP * 8 - RS * 4);
+                int pl = threadIdx.x / Q4, q = threadIdx.x % Q4;
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    cp16(smem_u32(reinterpret_cast<char *>(dst + pl * RSP) + tail + 16 * q), src + 4 * i);
+                    pl += dpl;
+                    q += dq;
+                    if (q >= Q4) { q -= Q4; pl++; }
                 }
             } else {
                 const int n = np * RS, dpl = blockDim.x / RS, drs = blockDim.x % RS;
@@ -116,8 +130,36 @@ __device__ __forceinline__ void ns_prefetch(const View &v, const DevOp &op, int 
     }
 }
 
-// Widen the FP32 values this thread copied by ns_prefetch (after its wait):
-// the same slots, in place.
+// Widen an FP32 tile copied row-wise (RS a multiple of 4, at most 256): a
+// warp per row reads the row's floats from the tail of its slot, then writes
+// the doubles from the slot's start (all reads of the row before any write).
+__device__ __forceinline__ void ns_widen_rows(const DevOp &op, int np, int RS, int RSP, double *A, double *B) {
+    const int lane = threadIdx.x & 31, Q4 = RS / 4, tail = RSP * 8 - RS * 4;
+    for (int c = 0; c < (op.kind == kIntInt ? 2 : op.kind == kIntTip ? 1 : 0); c++) {
+        double *X = c == 0 ? A : B;
+        for (int pl = threadIdx.x >> 5; pl < np; pl += blockDim.x >> 5) {
+            double *row = X + pl * RSP;
+            const float4 *f = reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(row) + tail);
+            float4 v0 = make_float4(0.f, 0.f, 0.f, 0.f), v1 = v0;
+            if (lane < Q4) v0 = f[lane];
+            if (lane + 32 < Q4) v1 = f[lane + 32];
+            __syncwarp();
+            double2 *d = reinterpret_cast<double2 *>(row);
+            if (lane < Q4) {
+                d[2 * lane] = make_double2((double)v0.x, (double)v0.y);
+                d[2 * lane + 1] = make_double2((double)v0.z, (double)v0.w);
+            }
+            if (lane + 32 < Q4) {
+                d[2 * lane + 64] = make_double2((double)v1.x, (double)v1.y);
+                d[2 * lane + 65] = make_double2((double)v1.z, (double)v1.w);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Widen the FP32 values this thread copied by ns_prefetch element-wise (RS
+// not a multiple of 4; after its wait): the same slots, in place.
 __device__ __forceinline__ void ns_widen(const DevOp &op, int np, int RS, int RSP, double *A, double *B) {
     const int n = np * RS, dpl = blockDim.x / RS, drs = blockDim.x % RS;
     for (int c = 0; c < (op.kind == kIntInt ? 2 : op.kind == kIntTip ? 1 : 0); c++) {
@@ -125,7 +167,14 @@ __device__ __forceinline__ void ns_widen(const DevOp &op, int np, int RS, int RS
         int pl = threadIdx.x / RS, rs = threadIdx.x % RS;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             double *e = dst + pl * RSP + rs;
-            *e = (double)*reinterpret_cast<const float *>(e);
+            // IEEE float -> double on the bit fields (exact); zero and subnormals converted
+            const unsigned int u = *reinterpret_cast<const unsigned int *>(e);
+            const unsigned int E = (u >> 23) & 0xffu;
+            *e = (E != 0u && E != 255u)
+                     ? __longlong_as_double((long long)(((unsigned long long)(u >> 31) << 63) |
+                                                        ((unsigned long long)(E + 896u) << 52) |
+                                                        ((unsigned long long)(u & 0x7fffffu) << 29)))
+                     : (double)__uint_as_float(u);
             pl += dpl;
             rs += drs;
             if (rs >= RS) { rs -= RS; pl++; }
@@ -302,7 +351,14 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int R
         }
         cp_commit();
         cp_wait<1>();
-        if (p0 >= v.kpad) ns_widen(op, np, RS, RSP, A, B);
+        if (p0 >= v.kpad) {
+            if (RS % 4 == 0) {
+                __syncthreads();  // the rows' floats, copied by other threads, in shared memory
+                ns_widen_rows(op, np, RS, RSP, A, B);
+            } else {
+                ns_widen(op, np, RS, RSP, A, B);
+            }
+        }
         __syncthreads();  // this tile's stage (and P) in shared memory
         double val[Q][F];
         if (worker) {

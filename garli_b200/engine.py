@@ -390,10 +390,10 @@ class Instance:
         _chk(lib().gb_set_kernel_timing(self.h, int(on)), "gb_set_kernel_timing")
 
     def kernel_timing(self) -> dict:
-        out = np.zeros(6)
+        out = np.zeros(7)
         _chk(lib().gb_get_kernel_timing(self.h, _p(out, C.c_double)), "gb_get_kernel_timing")
         return {"cla_ms": out[0], "cla_launches": int(out[1]), "pattern_updates": int(out[2]),
-                "edge_ms": out[3], "edge_evals": int(out[4]), "cla_bytes": out[5]}
+                "edge_ms": out[3], "edge_evals": int(out[4]), "cla_bytes": out[5], "cla_fp64_instr": out[6]}
 
     def synchronize(self):
         _chk(lib().gb_synchronize(self.h), "gb_synchronize")

@@ -199,8 +199,9 @@ int gb_synchronize(int instance);
 const char *gb_last_error(void);
 /* instrumentation: the instance's CUDA stream (cudaStream_t) and optional
  * CUDA-event timing of the CLA and edge kernels on that stream;
- * timing out[0..5] = CLA ms, CLA launches, pattern-updates, edge ms, edge evaluations,
- * algorithmic bytes of the timed CLA launches */
+ * timing out[0..6] = CLA ms, CLA launches, pattern-updates, edge ms, edge evaluations,
+ * algorithmic bytes of the timed CLA launches, FP64 instructions of the timed
+ * CLA launches (n-state CUDA-core kernel; 0 for 4 states) */
 int gb_get_stream(int instance, void **stream);
 int gb_set_kernel_timing(int instance, int on);
 int gb_get_kernel_timing(int instance, double *out);
