@@ -300,12 +300,35 @@ static dim3 ns_cla_grid(const Instance *I, void *f, size_t smem, int npat, int t
     const int per_op = std::max(1, occ * I->nsm / std::max(1, nops));
     return dim3(std::max(1, std::min(ntiles, per_op)), nops);
 }
+static void *ns_edge_func(int S, bool garli, bool deriv) {
+    if (S <= 20)
+        return garli ? (deriv ? (void *)k_edge_ns<true, true, 20> : (void *)k_edge_ns<true, false, 20>)
+                     : (deriv ? (void *)k_edge_ns<false, true, 20> : (void *)k_edge_ns<false, false, 20>);
+    return garli ? (deriv ? (void *)k_edge_ns<true, true, 61> : (void *)k_edge_ns<true, false, 61>)
+                 : (deriv ? (void *)k_edge_ns<false, true, 61> : (void *)k_edge_ns<false, false, 61>);
+}
+// pattern tile of k_edge_ns (as k_cla_ns: a power of two, at most one warp
+// task per warp, the derivative form within 200 KB) and its dynamic shared
+// memory (derivative form: the larger)
 static int ns_edge_tile(const Instance *I, size_t *smem) {
-    const int RS = I->R * I->S, RSS = RS * I->S;
+    const int pw = I->S <= 20 ? NsTile<20, kEdgeQ>::PW : NsTile<61, kEdgeQ>::PW;
     int tp = 64;
-    while (tp > 1 && (size_t)(3 * RSS + 5 * tp * RS + I->S + I->R) * 8 > 180 * 1024) tp >>= 1;
-    *smem = (size_t)(3 * RSS + 5 * tp * RS + I->S + I->R) * 8;
+    while (tp > pw && (I->R * (tp / pw) > kThreads / 32 || ns_edge_smem_bytes(I->S, I->R, tp, true) > 200 * 1024))
+        tp >>= 1;
+    *smem = ns_edge_smem_bytes(I->S, I->R, tp, true);
     return tp;
+}
+// blocks of an n-state edge evaluation: one resident wave (the derivative
+// form's occupancy), so that evaluations with and without derivatives sum
+// the same block partials
+static int ns_edge_blocks(const Instance *I, int tp, size_t smem) {
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ns_edge_func(I->S, !I->mixed, true), kThreads, smem) !=
+            cudaSuccess ||
+        occ < 1)
+        occ = 1;
+    const int ntiles = (I->npat + tp - 1) / tp;
+    return std::max(1, std::min(std::min(ntiles, occ * I->nsm), kMaxScoreBlocks));
 }
 
 // tensor-core CLA update (gb_tc.cuh): supported shapes and launch parameters.
@@ -353,10 +376,10 @@ static int set_smem_attrs() {
     for (int S : {20, 61})
         for (bool g : {true, false})
             GB_CUDA(cudaFuncSetAttribute(ns_cla_func(S, g), cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GB_CUDA(cudaFuncSetAttribute(k_edge_ns<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    for (int S : {20, 61})
+        for (bool g : {true, false})
+            for (bool d : {true, false})
+                GB_CUDA(cudaFuncSetAttribute(ns_edge_func(S, g, d), cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     GB_CUDA(cudaFuncSetAttribute(k_pmats, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     for (int R = 1; R <= 8; R++)
         GB_CUDA(cudaFuncSetAttribute(level4m_ops_func(R), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1178,15 +1201,12 @@ static int edge_enqueue(Instance *I, const gb_scoring_operation *op, int slot, d
         }
     } else {
         size_t smem;
-        const int tp = ns_edge_tile(I, &smem);
-        nblocks = std::min(kMaxScoreBlocks, (I->npat + tp - 1) / tp);
-        if (I->mixed) {
-            if (D) k_edge_ns<false, true><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
-            else k_edge_ns<false, false><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
-        } else {
-            if (D) k_edge_ns<true, true><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
-            else k_edge_ns<true, false><<<nblocks, kThreads, smem, I->stream>>>(v, pb, cidx, op->transMatIndex, tip, 1, I->S, I->R, tp);
-        }
+        int tp = ns_edge_tile(I, &smem);
+        nblocks = ns_edge_blocks(I, tp, smem);
+        int pbi = pb, cbi = cidx, mat = op->transMatIndex, tipi = tip, ws = 1, R = I->R;
+        void *args[] = {&v, &pbi, &cbi, &mat, &tipi, &ws, &R, &tp};
+        GB_CUDA(cudaLaunchKernel(ns_edge_func(I->S, !I->mixed, D), dim3(nblocks), dim3(kThreads), args, smem,
+                                 I->stream));
     }
     int rc = check_launch(I);
     if (rc) return rc;
@@ -1575,7 +1595,7 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
         ns_tp = ns_cla_tile(I, &ns_smem);
         ns_edge_tp = ns_edge_tile(I, &ns_edge_smem);
     }
-    const int nblocks = dna ? I->nvb4 : std::min(kMaxScoreBlocks, (I->npat + ns_edge_tp - 1) / ns_edge_tp);
+    const int nblocks = dna ? I->nvb4 : ns_edge_blocks(I, ns_edge_tp, ns_edge_smem);
     const size_t pmat_smem = pmat_smem_bytes(I->S, I->R);
     int rc;
     {
@@ -1656,10 +1676,9 @@ static int build_pass_graph(Instance *I, const gb_nr_branch *br, int nbr,
         } else {
             int ws = 0;
             {
-                int S = I->S, R = I->R, tp = ns_edge_tp;
-                void *args[] = {&v, &pb, &cb, &mat, &tip, &ws, &S, &R, &tp};
-                rc = B.add(body, &bprev, garli ? (void *)k_edge_ns<true, true> : (void *)k_edge_ns<false, true>,
-                           dim3(nblocks), ns_edge_smem, args);
+                int R = I->R, tp = ns_edge_tp;
+                void *args[] = {&v, &pb, &cb, &mat, &tip, &ws, &R, &tp};
+                rc = B.add(body, &bprev, ns_edge_func(I->S, garli, true), dim3(nblocks), ns_edge_smem, args);
                 if (rc) return rc;
             }
             {

@@ -34,14 +34,17 @@ __device__ __forceinline__ void tile_load(const View &v, int b, int p0, int RS, 
 // (fg, fg + NF, ...) of Q patterns (qg, qg + NQ, ...) of one rate category, so
 // each P entry read from shared memory serves Q patterns and each child value
 // serves F from-states.
-template <int S>
+template <int S, int QP = 2>
 struct NsTile {
     static constexpr int NF = S <= 20 ? 4 : 8;
     static constexpr int F = (S + NF - 1) / NF;
     static constexpr int NQ = 32 / NF;
-    static constexpr int Q = 2;
+    static constexpr int Q = QP;
     static constexpr int PW = NQ * Q;  // patterns of one warp task; tiles are multiples of it
 };
+// the edge kernel's tile (two patterns per lane measured faster than one
+// with two blocks per SM)
+constexpr int kEdgeQ = 2;
 
 // Row stride (in doubles) of a pattern in a child tile: >= RS and 2 mod 4,
 // so rows start 16-byte aligned and the 16-byte reads of one "to" pair by the
@@ -431,104 +434,223 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int R
     cp_wait<0>();
 }
 
-// Edge evaluation for S states: per-(pattern, rate, from) terms computed in
-// parallel, then summed per pattern in the reference's order.
-// dynamic smem: M[3*R*S*S], C[TP*R*S], Pp[TP*R*S], T[3*TP*R*S], freqs[S], rp[R]
-template <bool GARLI_SCALE, bool DERIV>
-__global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf, int mat, int child_tip,
-                                                      int write_sites, int S, int R, int TP) {
-    extern __shared__ double sm[];
-    const int RS = R * S, RSS = R * S * S, SS = S * S;
-    double *M = sm, *C = M + 3 * RSS, *Pp = C + TP * RS, *T = Pp + TP * RS, *F = T + 3 * TP * RS, *RP = F + S;
-    const double *mp = v.mats + (long long)mat * v.mat_stride;
-    // P, dP, d2P transposed, [matrix][rate][to][from]: the threads of a warp
-    // take consecutive "from" states, so each "to" step reads consecutive words
-    for (int i = threadIdx.x; i < (DERIV ? 3 : 1) * RSS; i += blockDim.x) {
-        const int k = i / RSS, j = i % RSS, r = j / SS, from = (j % SS) / S, to = j % S;
-        M[k * RSS + r * SS + to * S + from] = mp[i];
-    }
-    for (int i = threadIdx.x; i < S; i += blockDim.x) F[i] = v.freqs[i];
-    for (int i = threadIdx.x; i < R; i += blockDim.x) RP[i] = v.rate_probs[i];
+// dynamic shared memory of k_edge_ns in bytes: P (and dP, d2P) of the edge,
+// two stages of the parent's and the child's tiles, per-(sum, rate, pattern)
+// from-sums, frequencies and category probabilities, then per stage the
+// scalers, counts and constant states ([stage][4][TP] ints) and the child's
+// tip codes ([stage][2][TP] bytes, child in the second half)
+__host__ __device__ inline size_t ns_edge_smem_bytes(int S, int R, int TP, bool deriv) {
+    const size_t RS = (size_t)R * S, RSP = (size_t)ns_row_stride(R * S);
+    const size_t dbl = (deriv ? 3 : 1) * RS * S + 4 * (size_t)TP * RSP + 3 * (size_t)R * TP + S + R;
+    return (dbl * 8 + 15) / 16 * 16 + 2 * 4 * (size_t)TP * 4 + 2 * 2 * (size_t)TP;
+}
+
+// Edge evaluation for S states (the n-state forms of Tree::GetScore /
+// ConditionalLikelihoodRateHet, tree.cpp:5597-6460, and of the derivative
+// sums, optimization.cpp:2592-3614): per (pattern, rate, from) the child's
+// transition sum l = sum_to P[from][to] * child[to] (dP, d2P for the
+// derivatives; a tip child's entry directly), the term
+// l * partial[from] * freqs[from], summed over "from" in order per rate, then
+// over rates with the category probabilities, plus pinv, log and the
+// derivative ratios; per-block sums of count-weighted site values.  The
+// per-site arithmetic and order are GARLI's (plain form: separate products
+// and sums; precision form: fused multiply-add in the transition sums).
+// Structure as k_cla_ns: matrices staged once per block, pattern tiles walked
+// grid-stride and double-buffered by cp.async, one warp task (rate, PW
+// patterns) per warp with a register tile of F from-states x Q patterns; a
+// rate's "from" sum runs in order through warp shuffles.
+template <bool GARLI_SCALE, bool DERIV, int S>
+__global__ void __launch_bounds__(kThreads, 1) k_edge_ns(View v, int pbuf, int cbuf, int mat, int child_tip,
+                                                         int write_sites, int R, int TP) {
+    using T = NsTile<S, kEdgeQ>;
+    constexpr int NF = T::NF, F = T::F, NQ = T::NQ, Q = T::Q, SS = S * S, NM = DERIV ? 3 : 1;
+    extern __shared__ __align__(16) double sm[];
+    const int RS = R * S, RSS = R * SS, RSP = ns_row_stride(RS);
+    double *M = sm, *stg = M + NM * RSS, *rsum = stg + 4 * TP * RSP, *Fq = rsum + 3 * R * TP, *RP = Fq + S;
+    char *tail = reinterpret_cast<char *>(sm) +
+                 ((size_t)(NM * RSS + 4 * TP * RSP + 3 * R * TP + S + R) * 8 + 15) / 16 * 16;
+    int *scs = reinterpret_cast<int *>(tail);                  // [stage][parent, child, count, const][TP]
+    uint8_t *tts = reinterpret_cast<uint8_t *>(scs + 8 * TP);  // [stage][-, child][TP]
+    DevOp op;  // the parent as child 1 and the child as child 2 of a CLA op, for the staging helpers
+    op.c1 = pbuf;
+    op.c2 = cbuf;
+    op.kind = child_tip ? kIntTip : kIntInt;
+    const int ntiles = (v.npat + TP - 1) / TP;
+    auto prefetch = [&](int tile, int st) {
+        const int p0 = tile * TP, np = min(TP, v.npat - p0);
+        double *A = stg + st * 2 * TP * RSP;
+        int *sc = scs + st * 4 * TP;
+        ns_prefetch(v, op, p0, np, RS, RSP, TP, A, A + TP * RSP, sc, tts + st * 2 * TP);
+        for (int q = threadIdx.x; q < np; q += blockDim.x) {
+            cp4(smem_u32(sc + 2 * TP + q), v.counts + p0 + q);
+            cp4(smem_u32(sc + 3 * TP + q), v.const_states + p0 + q);
+        }
+    };
     double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
-    for (int p0 = blockIdx.x * TP; p0 < v.npat; p0 += gridDim.x * TP) {
-        const int np = min(TP, v.npat - p0);
-        __syncthreads();
-        tile_load(v, pbuf, p0, RS, np * RS, Pp);
-        if (!child_tip) tile_load(v, cbuf, p0, RS, np * RS, C);
-        __syncthreads();
-        for (int o = threadIdx.x; o < np * RS; o += blockDim.x) {
-            const int pl = o / RS, rem = o % RS, r = rem / S, from = rem % S;
-            const int p = p0 + pl;
-            const double *col = M + r * SS + from;  // P[from][to] = col[to * S]
-            double l = 0.0, a = 0.0, b = 0.0;
-            if (!child_tip) {
-                const double *c = C + pl * RS + r * S;
-                for (int to = 0; to < S; to++) {
-                    l = add(l, mul(col[to * S], c[to]));
-                    if (DERIV) {
-                        a = add(a, mul(col[RSS + to * S], c[to]));
-                        b = add(b, mul(col[2 * RSS + to * S], c[to]));
-                    }
-                }
+    if ((int)blockIdx.x < ntiles) {
+        prefetch(blockIdx.x, 0);
+        cp_commit();
+        const double *mp = v.mats + (long long)mat * v.mat_stride;
+        for (int i = threadIdx.x; i < NM * RSS; i += blockDim.x) M[i] = mp[i];
+        for (int i = threadIdx.x; i < S; i += blockDim.x) Fq[i] = v.freqs[i];
+        for (int i = threadIdx.x; i < R; i += blockDim.x) RP[i] = v.rate_probs[i];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int fg = lane % NF, qg = lane / NF;
+    const int tasks = R * (TP / T::PW);  // <= warps of the block (host-chosen TP)
+    const bool worker = warp < tasks;
+    const int r = worker ? warp % R : 0, pb = worker ? (warp / R) * T::PW : 0;
+    int fr[F], pl[Q];
+#pragma unroll
+    for (int k = 0; k < F; k++) fr[k] = min(fg + NF * k, S - 1);
+#pragma unroll
+    for (int j = 0; j < Q; j++) pl[j] = pb + qg + NQ * j;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int st = it & 1;
+        const int p0 = tile * TP, np = min(TP, v.npat - p0);
+        double *A = stg + st * 2 * TP * RSP, *B = A + TP * RSP;  // parent partial, child
+        const int *sc = scs + st * 4 * TP;
+        const uint8_t *tt = tts + st * 2 * TP;
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) prefetch(nxt, st ^ 1);
+        cp_commit();
+        cp_wait<1>();
+        if (p0 >= v.kpad) {
+            if (RS % 4 == 0) {
+                __syncthreads();
+                ns_widen_rows(op, np, RS, RSP, A, B);
             } else {
-                const int s = v.tips[(long long)cbuf * v.npat_pad + p];
-                if (s < S) {
-                    l = col[s * S];
-                    if (DERIV) {
-                        a = col[RSS + s * S];
-                        b = col[2 * RSS + s * S];
+                ns_widen(op, np, RS, RSP, A, B);
+            }
+        }
+        __syncthreads();  // this tile's stage (and the matrices) in shared memory
+        if (worker) {
+            const double *m0 = M + r * SS;
+            double tl[Q][F], t1[Q][F], t2[Q][F];
+            if (!child_tip) {
+                double l[Q][F], a[Q][F], b[Q][F];
+#pragma unroll
+                for (int j = 0; j < Q; j++)
+#pragma unroll
+                    for (int k = 0; k < F; k++) l[j][k] = a[j][k] = b[j][k] = 0.0;
+                const double *Br = B + r * S;
+                if constexpr (S % 2 == 0) {
+#pragma unroll 1
+                    for (int to = 0; to < S; to += 2) {
+                        double2 c[Q];
+#pragma unroll
+                        for (int j = 0; j < Q; j++) c[j] = *reinterpret_cast<const double2 *>(Br + pl[j] * RSP + to);
+#pragma unroll
+                        for (int k = 0; k < F; k++) {
+                            const double2 p = *reinterpret_cast<const double2 *>(m0 + fr[k] * S + to);
+#pragma unroll
+                            for (int j = 0; j < Q; j++) {
+                                l[j][k] = mac<!GARLI_SCALE>(l[j][k], p.x, c[j].x);
+                                l[j][k] = mac<!GARLI_SCALE>(l[j][k], p.y, c[j].y);
+                            }
+                            if (DERIV) {
+                                const double2 p1 = *reinterpret_cast<const double2 *>(m0 + RSS + fr[k] * S + to);
+                                const double2 p2 = *reinterpret_cast<const double2 *>(m0 + 2 * RSS + fr[k] * S + to);
+#pragma unroll
+                                for (int j = 0; j < Q; j++) {
+                                    a[j][k] = mac<!GARLI_SCALE>(a[j][k], p1.x, c[j].x);
+                                    a[j][k] = mac<!GARLI_SCALE>(a[j][k], p1.y, c[j].y);
+                                    b[j][k] = mac<!GARLI_SCALE>(b[j][k], p2.x, c[j].x);
+                                    b[j][k] = mac<!GARLI_SCALE>(b[j][k], p2.y, c[j].y);
+                                }
+                            }
+                        }
                     }
                 } else {
-                    l = 1.0;  // total ambiguity: partial*freq only, no derivative terms
+#pragma unroll 1
+                    for (int to = 0; to < S; to++) {
+                        double c[Q];
+#pragma unroll
+                        for (int j = 0; j < Q; j++) c[j] = Br[pl[j] * RSP + to];
+#pragma unroll
+                        for (int k = 0; k < F; k++) {
+                            const double p = m0[fr[k] * S + to];
+#pragma unroll
+                            for (int j = 0; j < Q; j++) l[j][k] = mac<!GARLI_SCALE>(l[j][k], p, c[j]);
+                            if (DERIV) {
+                                const double p1 = m0[RSS + fr[k] * S + to], p2 = m0[2 * RSS + fr[k] * S + to];
+#pragma unroll
+                                for (int j = 0; j < Q; j++) {
+                                    a[j][k] = mac<!GARLI_SCALE>(a[j][k], p1, c[j]);
+                                    b[j][k] = mac<!GARLI_SCALE>(b[j][k], p2, c[j]);
+                                }
+                            }
+                        }
+                    }
+                }
+                // reference: temp * partial[from] * freqs[from]
+#pragma unroll
+                for (int j = 0; j < Q; j++)
+#pragma unroll
+                    for (int k = 0; k < F; k++) {
+                        const double w = A[pl[j] * RSP + r * S + fr[k]], f = Fq[fr[k]];
+                        tl[j][k] = mul(mul(l[j][k], w), f);
+                        t1[j][k] = DERIV ? mul(mul(a[j][k], w), f) : 0.0;
+                        t2[j][k] = DERIV ? mul(mul(b[j][k], w), f) : 0.0;
+                    }
+            } else {
+#pragma unroll
+                for (int j = 0; j < Q; j++) {
+                    const int s = tt[TP + pl[j]];
+#pragma unroll
+                    for (int k = 0; k < F; k++) {
+                        const double w = A[pl[j] * RSP + r * S + fr[k]], f = Fq[fr[k]];
+                        if (s < S) {
+                            tl[j][k] = mul(mul(m0[fr[k] * S + s], w), f);
+                            t1[j][k] = DERIV ? mul(mul(m0[RSS + fr[k] * S + s], w), f) : 0.0;
+                            t2[j][k] = DERIV ? mul(mul(m0[2 * RSS + fr[k] * S + s], w), f) : 0.0;
+                        } else {
+                            // total ambiguity: partial[from] * freqs[from], no derivative terms
+                            tl[j][k] = mul(w, f);
+                            t1[j][k] = DERIV ? mul(mul(0.0, w), f) : 0.0;
+                            t2[j][k] = DERIV ? mul(mul(0.0, w), f) : 0.0;
+                        }
+                    }
                 }
             }
-            const double w = Pp[pl * RS + r * S + from];
-            const bool amb = child_tip && v.tips[(long long)cbuf * v.npat_pad + p] >= S;
-            // reference: temp * partial[from] * freqs[from]  (ambiguous tip: partial[from] * freqs[from])
-            T[o] = amb ? mul(w, F[from]) : mul(mul(l, w), F[from]);
-            if (DERIV) {
-                T[TP * RS + o] = mul(mul(a, w), F[from]);
-                T[2 * TP * RS + o] = mul(mul(b, w), F[from]);
+            // this rate's sums over "from", in order: the value of "from" lives in
+            // lane (qg, from % NF), register from / NF
+#pragma unroll
+            for (int j = 0; j < Q; j++) {
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int from = 0; from < S; from++) {
+                    const int src = qg * NF + from % NF;
+                    s0 = add(s0, __shfl_sync(0xffffffffu, tl[j][from / NF], src));
+                    if (DERIV) {
+                        s1 = add(s1, __shfl_sync(0xffffffffu, t1[j][from / NF], src));
+                        s2 = add(s2, __shfl_sync(0xffffffffu, t2[j][from / NF], src));
+                    }
+                }
+                if (fg == 0) {
+                    rsum[r * TP + pl[j]] = s0;
+                    rsum[(R + r) * TP + pl[j]] = s1;
+                    rsum[(2 * R + r) * TP + pl[j]] = s2;
+                }
             }
         }
         __syncthreads();
-        for (int pl = threadIdx.x; pl < np; pl += blockDim.x) {
-            const int p = p0 + pl;
+        for (int q = threadIdx.x; q < np; q += blockDim.x) {
+            const int p = p0 + q;
             double siteL = 0.0, sD1 = 0.0, sD2 = 0.0;
-            if (R == 1) {
-                for (int from = 0; from < S; from++) {
-                    siteL = add(siteL, T[pl * RS + from]);
-                    if (DERIV) {
-                        sD1 = add(sD1, T[TP * RS + pl * RS + from]);
-                        sD2 = add(sD2, T[2 * TP * RS + pl * RS + from]);
-                    }
-                }
-                siteL = mul(siteL, RP[0]);
+            for (int rr = 0; rr < R; rr++) {
+                siteL = add(siteL, mul(rsum[rr * TP + q], RP[rr]));
                 if (DERIV) {
-                    sD1 = mul(sD1, RP[0]);
-                    sD2 = mul(sD2, RP[0]);
-                }
-            } else {
-                for (int r = 0; r < R; r++) {
-                    double rL = 0.0, r1 = 0.0, r2 = 0.0;
-                    for (int from = 0; from < S; from++) {
-                        rL = add(rL, T[pl * RS + r * S + from]);
-                        if (DERIV) {
-                            r1 = add(r1, T[TP * RS + pl * RS + r * S + from]);
-                            r2 = add(r2, T[2 * TP * RS + pl * RS + r * S + from]);
-                        }
-                    }
-                    siteL = add(siteL, mul(rL, RP[r]));
-                    if (DERIV) {
-                        sD1 = add(sD1, mul(r1, RP[r]));
-                        sD2 = add(sD2, mul(r2, RP[r]));
-                    }
+                    sD1 = add(sD1, mul(rsum[(R + rr) * TP + q], RP[rr]));
+                    sD2 = add(sD2, mul(rsum[(2 * R + rr) * TP + q], RP[rr]));
                 }
             }
-            const int m1 = v.scalers[(long long)pbuf * v.npat_pad + p];
-            const int m2 = child_tip ? 0 : v.scalers[(long long)cbuf * v.npat_pad + p];
-            if (v.has_pinv && v.const_states[p] >= 0) {
-                const double pf = mul(v.pinv, F[v.const_states[p]]);
+            const int m1 = sc[q];
+            const int m2 = child_tip ? 0 : sc[TP + q];
+            const int cs = sc[3 * TP + q];
+            if (v.has_pinv && cs >= 0) {
+                const double pf = mul(v.pinv, Fq[cs]);
                 if (GARLI_SCALE) {
                     if (DERIV) {
                         // prI*freq*exp(partial)*exp(child) (optimization.cpp:3300, :3507)
@@ -558,7 +680,7 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
             }
             // GARLI drops non-negative site lnLs (tree.cpp:6380, optimization.cpp:3378)
             if (u < 0.0) {
-                const double cnt = (double)v.counts[p];
+                const double cnt = (double)sc[2 * TP + q];
                 accL = add(accL, mul(u, cnt));
                 if (DERIV) {
                     acc1 = add(acc1, mul(cnt, d1));
@@ -566,8 +688,9 @@ __global__ void __launch_bounds__(kThreads) k_edge_ns(View v, int pbuf, int cbuf
                 }
             }
         }
+        __syncthreads();  // the stage's scalers read before the next prefetch overwrites them
     }
-    __syncthreads();
+    cp_wait<0>();
     block_sum3(accL, acc1, acc2, v.block_sums + 3 * blockIdx.x);
 }
 

@@ -159,6 +159,31 @@ def test_nstate_synthetic(kind):
         assert np.allclose(g, o, rtol=1e-8, atol=1e-8)
 
 
+@pytest.mark.parametrize("ncat", [1, 3, 8])
+def test_nstate_category_counts(ncat):
+    """20 states with 1, 3 and 8 rate categories: the CUDA-core CLA kernel's
+    tile holds one warp task per (category, 16 patterns), so the category
+    count sets the tile (64, 32, 16 patterns) and the idle warps.  Plain form
+    against the oracle at 1e-8, precision form (CUDA cores) at 1e-4."""
+    rng = np.random.default_rng(40 + ncat)
+    c3, dl = synth.yule_tree(14, rng, 0.15)
+    spec = synth.aa_spec(rng, 0.7, ncat)
+    m = synth.build_model(spec)
+    w = synth.Workload(f"aa_{ncat}", c3, dl, m, synth.compress(synth.simulate(c3, dl, m, 700, rng), 20), spec)
+    inst, tree, ot = _both(w.data, c3, dl, m, omodel=w.model_with(orc))
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
+    for nd in (1, w.data.ntax + 2):
+        assert np.allclose(tree.derivatives(nd), ot.derivatives(nd), rtol=1e-8, atol=1e-8)
+    tree.close()
+    inst.close()
+    inst, tree = engine.tree_engine(w.data, c3, dl, m, mixed=True)
+    inst.set_tensor_cores(False)
+    assert abs(tree.score(0) - lo) <= 1e-4
+    tree.close()
+    inst.close()
+
+
 @pytest.mark.parametrize("name", PINS)
 def test_mixed_precision_form(name):
     fx, pd, c3, dl = load_fixture(name)
