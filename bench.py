@@ -408,7 +408,8 @@ def nstate_forms(kind, device, reps=3, tile=0):
     """Secondary: full-tree rescore of the 20-state (64 taxa x 20,000 sites, +G4)
     or 61-state (32 taxa x 5,000 codons) alignment in the precision form with the
     tensor-core CLA update, the same form on CUDA cores, and the plain FP64 form;
-    CLA site-updates/s (device-timed) and each form's lnL against plain FP64."""
+    CLA site-updates/s (device-timed) and each form's lnL against plain FP64;
+    then one all-branch Newton pass per form (device-timed)."""
     import torch
 
     from garli_b200 import engine, synth
@@ -457,6 +458,22 @@ def nstate_forms(kind, device, reps=3, tile=0):
             ips = kt["cla_fp64_instr"] / (kt["cla_ms"] / 1000.0)
             out[name]["cla_fp64_instr_per_s"] = ips
             out[name]["cla_fp64_frac_of_nominal"] = ips / fp64_nominal_instr_per_s()
+        # one all-branch Newton pass (OptimizeAllBranches, GARLI's branch order and
+        # precision 0.01) from the starting lengths, device-timed: CLA updates,
+        # edge derivatives, Newton steps; the first pass (untimed) builds the
+        # pass's device schedule
+        for timed in (False, True):
+            for nd in range(1, len(w.dlen)):
+                tree.set_branch_length(nd, float(w.dlen[nd]))
+            tree.make_all_dirty()
+            tree.score(0)
+            torch.cuda.synchronize(device)
+            e0.record(stream)
+            imp, lnl_after = tree.optimize_all_branches(0.01)
+            e1.record(stream)
+            torch.cuda.synchronize(device)
+        out[name]["newton_pass_ms"] = e0.elapsed_time(e1)
+        out[name]["newton_pass_lnl"] = lnl_after
         tree.close()
         inst.close()
     return out
