@@ -300,6 +300,9 @@ static dim3 ns_cla_grid(const Instance *I, void *f, size_t smem, int npat, int t
     const int per_op = std::max(1, occ * I->nsm / std::max(1, nops));
     return dim3(std::max(1, std::min(ntiles, per_op)), nops);
 }
+// opt-in dynamic shared memory of the n-state edge kernel (the device's 227 KB
+// per block less the kernel's static reduction array)
+constexpr int kEdgeSmemMax = 227 * 1024 - 1024;
 static void *ns_edge_func(int S, bool garli, bool deriv) {
     if (S <= 20)
         return garli ? (deriv ? (void *)k_edge_ns<true, true, 20> : (void *)k_edge_ns<true, false, 20>)
@@ -315,6 +318,7 @@ static int ns_edge_tile(const Instance *I, size_t *smem) {
     int tp = 64;
     while (tp > pw && (I->R * (tp / pw) > kThreads / 32 || ns_edge_smem_bytes(I->S, I->R, tp, true) > 200 * 1024))
         tp >>= 1;
+    // 61 states with 2 categories hold 179 KB of matrices: up to the opt-in limit (kEdgeSmemMax)
     *smem = ns_edge_smem_bytes(I->S, I->R, tp, true);
     return tp;
 }
@@ -379,7 +383,8 @@ static int set_smem_attrs() {
     for (int S : {20, 61})
         for (bool g : {true, false})
             for (bool d : {true, false})
-                GB_CUDA(cudaFuncSetAttribute(ns_edge_func(S, g, d), cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+                GB_CUDA(cudaFuncSetAttribute(ns_edge_func(S, g, d), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kEdgeSmemMax));
     GB_CUDA(cudaFuncSetAttribute(k_pmats, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     for (int R = 1; R <= 8; R++)
         GB_CUDA(cudaFuncSetAttribute(level4m_ops_func(R), cudaFuncAttributeMaxDynamicSharedMemorySize,

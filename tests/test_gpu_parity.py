@@ -184,6 +184,25 @@ def test_nstate_category_counts(ncat):
     inst.close()
 
 
+def test_codon_two_categories():
+    """61 states with 2 rate categories: the edge kernel's matrices (P, dP,
+    d2P: 179 KB) fill most of shared memory and the tiles shrink to one warp
+    task per category.  Plain form against the oracle at 1e-8."""
+    rng = np.random.default_rng(61)
+    c3, dl = synth.yule_tree(10, rng, 0.2)
+    base = synth.codon_spec(rng)
+    spec = synth.ModelSpec("codon", base.pi, None, 0.6, 2, None, base.kappa, base.omega)
+    m = synth.build_model(spec)
+    w = synth.Workload("codon_2", c3, dl, m, synth.compress(synth.simulate(c3, dl, m, 300, rng), 61), spec)
+    inst, tree, ot = _both(w.data, c3, dl, m, omodel=w.model_with(orc))
+    lg, lo = tree.score(0), ot.score(0)
+    assert abs(lg - lo) <= 1e-8 * abs(lo)
+    for nd in (1, w.data.ntax + 2):
+        assert np.allclose(tree.derivatives(nd), ot.derivatives(nd), rtol=1e-8, atol=1e-8)
+    tree.close()
+    inst.close()
+
+
 @pytest.mark.parametrize("name", PINS)
 def test_mixed_precision_form(name):
     fx, pd, c3, dl = load_fixture(name)
