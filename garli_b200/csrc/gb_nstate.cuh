@@ -64,6 +64,16 @@ __device__ __forceinline__ void cp8(uint32_t dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
 }
 
+// Asynchronous copy of n doubles (a block's matrices) into shared memory:
+// 16-byte pieces when both addresses are 16-byte aligned and n is even.
+__device__ __forceinline__ void stage_doubles(double *dst, const double *src, int n) {
+    if (((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15u) == 0 && n % 2 == 0) {
+        for (int i = threadIdx.x; i < n / 2; i += blockDim.x) cp16(smem_u32(dst + 2 * i), src + 2 * i);
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) cp8(smem_u32(dst + i), src + i);
+    }
+}
+
 // Asynchronous copy of one tile's inputs into a stage: the children's np
 // patterns x RS values pattern-major in rows of RSP doubles (FP64 tiles in
 // 16-byte pieces when RS is even; FP32 tiles, to be widened after the wait,
@@ -322,13 +332,9 @@ __global__ void __launch_bounds__(kThreads) k_cla_ns(View v, LevelOps ops, int R
     if ((int)blockIdx.x >= ntiles) return;
     ns_prefetch(v, op, blockIdx.x * TP, min(TP, plim - (int)blockIdx.x * TP), RS, RSP, TP, stg, stg + TP * RSP, scs,
                 tts);
+    stage_doubles(PL, v.mats + (long long)op.p1 * v.mat_stride, RSS);
+    stage_doubles(PR, v.mats + (long long)op.p2 * v.mat_stride, RSS);
     cp_commit();
-    const double *m1 = v.mats + (long long)op.p1 * v.mat_stride;
-    const double *m2 = v.mats + (long long)op.p2 * v.mat_stride;
-    for (int i = threadIdx.x; i < RSS; i += blockDim.x) {
-        PL[i] = m1[i];
-        PR[i] = m2[i];
-    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int fg = lane % NF, qg = lane / NF;
     const int tasks = R * (TP / T::PW);  // <= warps of the block (host-chosen TP)
@@ -489,9 +495,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_edge_ns(View v, int pbuf, int c
     double accL = 0.0, acc1 = 0.0, acc2 = 0.0;
     if ((int)blockIdx.x < ntiles) {
         prefetch(blockIdx.x, 0);
+        stage_doubles(M, v.mats + (long long)mat * v.mat_stride, NM * RSS);
         cp_commit();
-        const double *mp = v.mats + (long long)mat * v.mat_stride;
-        for (int i = threadIdx.x; i < NM * RSS; i += blockDim.x) M[i] = mp[i];
         for (int i = threadIdx.x; i < S; i += blockDim.x) Fq[i] = v.freqs[i];
         for (int i = threadIdx.x; i < R; i += blockDim.x) RP[i] = v.rate_probs[i];
     }
