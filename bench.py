@@ -458,6 +458,17 @@ def nstate_forms(kind, device, reps=3, tile=0):
             ips = kt["cla_fp64_instr"] / (kt["cla_ms"] / 1000.0)
             out[name]["cla_fp64_instr_per_s"] = ips
             out[name]["cla_fp64_frac_of_nominal"] = ips / fp64_nominal_instr_per_s()
+        # edge evaluation with first and second derivatives (the Newton step's
+        # input), its kernels device-timed over 20 calls
+        nd = w.data.ntax + 3
+        tree.derivatives(nd)
+        inst.set_kernel_timing(True)
+        for _ in range(20):
+            tree.derivatives(nd)
+        inst.synchronize()
+        kt = inst.kernel_timing()
+        inst.set_kernel_timing(False)
+        out[name]["edge_derivatives_us"] = kt["edge_ms"] * 1e3 / max(1, kt["edge_evals"])
         # one all-branch Newton pass (OptimizeAllBranches, GARLI's branch order and
         # precision 0.01) from the starting lengths, device-timed: CLA updates,
         # edge derivatives, Newton steps; the first pass (untimed) builds the
