@@ -5,29 +5,15 @@
 // :5597-6460, optimization.cpp:2592-3614).  CLA updates: a block stages the
 // op's two P(t) sets in shared memory once and walks pattern tiles, the next
 // tile's inputs arriving by cp.async while a register tile per lane (several
-// patterns x several from-states) is computed.  Edge evaluations: a block
-// owns a tile of patterns, one (pattern, rate, from) term per thread, summed
-// per pattern in the reference's order.
+// patterns x several from-states) is computed.  Edge evaluations: the same
+// structure with the edge's P, dP, d2P; each rate's sum over "from" runs in
+// the reference's order through warp shuffles.
 #pragma once
 #include "gb_common.cuh"
 #include "gb_dna.cuh"
 #include "gb_stage.cuh"
 
 namespace gb {
-
-template <typename ST>
-__device__ __forceinline__ double ldv(const ST *p) { return (double)__ldg(p); }
-
-// copy n consecutive CLA values of buffer b starting at pattern p0 into shared memory
-__device__ __forceinline__ void tile_load(const View &v, int b, int p0, int RS, int n, double *dst) {
-    if (p0 < v.kpad) {
-        const double *src = cla_ptr<double>(v, b, p0, RS);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = ldv<double>(src + i);
-    } else {
-        const float *src = cla_ptr<float>(v, b, p0, RS);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = ldv<float>(src + i);
-    }
-}
 
 // Register tile of the n-state CLA kernel: the 32 lanes of a warp are NF
 // "from"-state groups x NQ pattern groups; a lane computes F from-states
