@@ -132,6 +132,13 @@ struct Instance {
     // per-tree precision 4-state level launch aims at, patterns per block of
     // the n-state CUDA-core CLA kernel; 0 = the built-in choice
     int lvl_target = 0, ns_tp = 0;
+    // resident blocks per SM of a kernel at a dynamic shared memory size (queried once)
+    struct Occ {
+        const void *f;
+        size_t smem;
+        int blocks;
+    };
+    std::vector<Occ> occ_cache;
     bool tune_pending = true;
     // scratch of gb_set_eigen_from_rate_matrices, kept between calls
     double *d_eq = nullptr, *d_epi = nullptr;
@@ -293,9 +300,16 @@ static void *ns_cla_func(int S, bool garli) {
 }
 // blocks per op: at most one resident wave over all ops of the launch, each
 // block walking its op's tiles (P staged once per block)
-static dim3 ns_cla_grid(const Instance *I, void *f, size_t smem, int npat, int tp, int nops) {
+static int occupancy(Instance *I, const void *f, size_t smem) {
+    for (const auto &o : I->occ_cache)
+        if (o.f == f && o.smem == smem) return o.blocks;
     int occ = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kThreads, smem) != cudaSuccess || occ < 1) occ = 1;
+    I->occ_cache.push_back({f, smem, occ});
+    return occ;
+}
+static dim3 ns_cla_grid(Instance *I, void *f, size_t smem, int npat, int tp, int nops) {
+    const int occ = occupancy(I, f, smem);
     const int ntiles = (npat + tp - 1) / tp;
     const int per_op = std::max(1, occ * I->nsm / std::max(1, nops));
     return dim3(std::max(1, std::min(ntiles, per_op)), nops);
@@ -325,12 +339,8 @@ static int ns_edge_tile(const Instance *I, size_t *smem) {
 // blocks of an n-state edge evaluation: one resident wave (the derivative
 // form's occupancy), so that evaluations with and without derivatives sum
 // the same block partials
-static int ns_edge_blocks(const Instance *I, int tp, size_t smem) {
-    int occ = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ns_edge_func(I->S, !I->mixed, true), kThreads, smem) !=
-            cudaSuccess ||
-        occ < 1)
-        occ = 1;
+static int ns_edge_blocks(Instance *I, int tp, size_t smem) {
+    const int occ = occupancy(I, ns_edge_func(I->S, !I->mixed, true), smem);
     const int ntiles = (I->npat + tp - 1) / tp;
     return std::max(1, std::min(std::min(ntiles, occ * I->nsm), kMaxScoreBlocks));
 }
