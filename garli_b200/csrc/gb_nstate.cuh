@@ -46,10 +46,6 @@ __host__ __device__ inline size_t ns_cla_smem_bytes(int S, int R, int TP) {
     return (dbl * 8 + 15) / 16 * 16 + 2 * 2 * (size_t)TP * 4 + 2 * 2 * (size_t)TP;
 }
 
-__device__ __forceinline__ void cp8(uint32_t dst, const void *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
-}
-
 // Asynchronous copy of n doubles (a block's matrices) into shared memory:
 // 16-byte pieces when both addresses are 16-byte aligned and n is even.
 __device__ __forceinline__ void stage_doubles(double *dst, const double *src, int n) {

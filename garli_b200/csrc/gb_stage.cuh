@@ -42,6 +42,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
 __device__ __forceinline__ void cp16(uint32_t dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
+// 8-byte asynchronous copy global -> shared (both addresses 8-byte aligned)
+__device__ __forceinline__ void cp8(uint32_t dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
 // 4-byte asynchronous copy global -> shared (both addresses 4-byte aligned)
 __device__ __forceinline__ void cp4(uint32_t dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
